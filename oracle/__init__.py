@@ -1,0 +1,266 @@
+"""CPU oracle for the MAISE neural-network potential path (test infrastructure).
+
+Two checkers live here:
+
+* ``Oracle`` -- the C restatement in ``oracle/oracle.c`` (built into
+  ``oracle/liboracle.so`` by ``make -C oracle``), which restates the reference
+  algorithm in plain FP64 C and materialises the reference's derivative
+  blocks.
+* ``RefOracle`` -- the reference MAISE sources themselves, compiled by
+  ``make -C oracle ref`` into ``oracle/_ref/libmaise_ref.so`` with a GSL
+  stand-in.  It exists only where the reference sources were available at
+  build time.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may import this package.  The product (``maise_b200``) never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmaise_ref.so")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_L = ctypes.POINTER(ctypes.c_long)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_I)
+
+
+def build(ref: bool = True) -> None:
+    """Compile the restatement (and the reference, when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if ref and os.path.isdir(os.environ.get("MAISE_REFERENCE", "/root/reference")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8",
+                        "REF=" + os.environ.get("MAISE_REFERENCE", "/root/reference")], check=True)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+class Oracle:
+    """ctypes view of oracle/liboracle.so for one model file."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not os.path.exists(ORACLE_SO):
+                build(ref=False)
+            lib = ctypes.CDLL(ORACLE_SO)
+            lib.orc_model_load.restype = ctypes.c_void_p
+            lib.orc_model_load.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+            lib.orc_model_free.argtypes = [ctypes.c_void_p]
+            lib.orc_model_info.argtypes = [ctypes.c_void_p, _I, _I, _I, _D, _I, _I]
+            common = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I, _D, _D]
+            lib.orc_nlist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D,
+                                      ctypes.c_double, _I, _I, _I, _D]
+            lib.orc_descriptors_api.argtypes = common + [_D]
+            lib.orc_fn_api.argtypes = common + [ctypes.c_int, _I, _I, _D, _D]
+            lib.orc_vjp_api.argtypes = common + [_D, _D, _D]
+            lib.orc_efs_api.argtypes = common + [ctypes.c_double, ctypes.c_double, ctypes.c_int, _D, _D, _D, _D, _D]
+            lib.orc_cell_volume.restype = ctypes.c_double
+            lib.orc_cell_volume.argtypes = [_D]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, model_path: str):
+        err = ctypes.create_string_buffer(512)
+        self.h = self.lib().orc_model_load(model_path.encode(), err)
+        if not self.h:
+            raise ValueError(err.value.decode())
+        nspc, D, ng2, ng4 = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        spcz = (ctypes.c_int * 10)()
+        rc = ctypes.c_double()
+        self.lib().orc_model_info(self.h, ctypes.byref(nspc), ctypes.byref(D), spcz, ctypes.byref(rc),
+                                  ctypes.byref(ng2), ctypes.byref(ng4))
+        self.nspc, self.D, self.rc = nspc.value, D.value, rc.value
+        self.ng2, self.ng4 = ng2.value, ng4.value
+        self.spcz = list(spcz)[: self.nspc]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib().orc_model_free(self.h)
+            self.h = None
+
+    @staticmethod
+    def _prep(X, LAT, atmn):
+        X = np.ascontiguousarray(np.asarray(X, np.float64).reshape(-1)).copy()
+        LAT = np.ascontiguousarray(np.asarray(LAT, np.float64).reshape(9))
+        atmn = np.ascontiguousarray(np.asarray(atmn, np.int32))
+        return X, LAT, atmn
+
+    def nlist(self, X, LAT, atmn, ND, NM=512, rc=0.0):
+        X, LAT, atmn = self._prep(X, LAT, atmn)
+        N = len(atmn)
+        nn = np.zeros(N, np.int32)
+        nj = np.zeros(N * NM, np.int32)
+        nic = np.zeros(N * NM * 3, np.int32)
+        nr = np.zeros(N * NM)
+        rv = self.lib().orc_nlist(self.h, N, NM, ND, _dp(LAT), _dp(X), rc, _ip(nn), _ip(nj), _ip(nic), _dp(nr))
+        if rv:
+            raise RuntimeError("neighbour overflow")
+        return nn, nj.reshape(N, NM), nic.reshape(N, NM, 3), nr.reshape(N, NM), X.reshape(N, 3)
+
+    def descriptors(self, X, LAT, atmn, ND, NM=512):
+        X, LAT, atmn = self._prep(X, LAT, atmn)
+        N = len(atmn)
+        G = np.zeros(N * self.D)
+        if self.lib().orc_descriptors_api(self.h, N, NM, ND, _ip(atmn), _dp(LAT), _dp(X), _dp(G)):
+            raise RuntimeError("neighbour overflow")
+        return G.reshape(N, self.D)
+
+    def fn(self, X, LAT, atmn, ND, atom, NM=512):
+        """Derivative blocks of one atom: (dni, Fn[dnn+1, D, 3], Sn[D, 6])."""
+        X, LAT, atmn = self._prep(X, LAT, atmn)
+        N = len(atmn)
+        dnn = ctypes.c_int()
+        dni = np.zeros(NM + 1, np.int32)
+        Fn = np.zeros((NM + 1) * self.D * 3)
+        Sn = np.zeros(self.D * 6)
+        if self.lib().orc_fn_api(self.h, N, NM, ND, _ip(atmn), _dp(LAT), _dp(X), atom, ctypes.byref(dnn),
+                                 _ip(dni), _dp(Fn), _dp(Sn)):
+            raise RuntimeError("neighbour overflow")
+        k = dnn.value
+        return dni[:k].copy(), Fn[: (k + 1) * self.D * 3].reshape(k + 1, self.D, 3), Sn.reshape(self.D, 6)
+
+    def vjp(self, X, LAT, atmn, ND, g, NM=512):
+        X, LAT, atmn = self._prep(X, LAT, atmn)
+        N = len(atmn)
+        g = np.ascontiguousarray(np.asarray(g, np.float64).reshape(N * self.D))
+        F = np.zeros(3 * N)
+        U = np.zeros(6)
+        if self.lib().orc_vjp_api(self.h, N, NM, ND, _ip(atmn), _dp(LAT), _dp(X), _dp(g), _dp(F), _dp(U)):
+            raise RuntimeError("neighbour overflow")
+        return F.reshape(N, 3), U
+
+    def efs(self, X, LAT, atmn, ND, urep=0.0, p_gpa=0.0, forces=True, NM=512):
+        """dict(E, H, EA, F, U, X) following CELL_FRC / CELL_ENE."""
+        X, LAT, atmn = self._prep(X, LAT, atmn)
+        N = len(atmn)
+        E, H = ctypes.c_double(), ctypes.c_double()
+        EA = np.zeros(N)
+        F = np.zeros(3 * N)
+        U = np.zeros(6)
+        if self.lib().orc_efs_api(self.h, N, NM, ND, _ip(atmn), _dp(LAT), _dp(X), urep, p_gpa, int(forces),
+                                  ctypes.byref(E), ctypes.byref(H), _dp(EA), _dp(F), _dp(U)):
+            raise RuntimeError("neighbour overflow")
+        return dict(E=E.value, H=H.value, EA=EA, F=F.reshape(N, 3), U=U, X=X.reshape(N, 3))
+
+
+class RefOracle:
+    """ctypes view of the reference sources compiled under oracle/_ref.
+
+    The reference keeps global state (one model at a time, arrays sized by the
+    first call); the harness re-initialises when the model directory changes
+    or a larger structure arrives.  model_dir must hold a file named 'model'.
+    """
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not ref_available():
+                raise FileNotFoundError("oracle/_ref/libmaise_ref.so was not built (needs the reference sources)")
+            lib = ctypes.CDLL(REF_SO)
+            c_i, c_d = ctypes.c_int, ctypes.c_double
+            lib.ref_efs.restype = c_d
+            lib.ref_efs.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, _D, _D, _D, _D]
+            lib.ref_energy.restype = c_d
+            lib.ref_energy.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, c_d, c_d]
+            lib.ref_descriptors.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, _D]
+            lib.ref_fn.argtypes = [c_i, _I, _I, _D, _D]
+            lib.ref_positions.argtypes = [c_i, _D]
+            lib.ref_relax.restype = c_d
+            lib.ref_relax.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _L]
+            lib.ref_nvt.restype = c_d
+            lib.ref_nvt.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, _D, c_i, ctypes.c_long, c_d,
+                                    c_d, c_d, c_i, c_d, _D, _D]
+            lib.ref_maxwell.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, ctypes.c_long, c_d, _D]
+            lib.ref_sizes.argtypes = [_I]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, model_dir: str, nthreads: int = 0):
+        self.dir = os.path.abspath(model_dir).encode()
+        self.np = nthreads or os.cpu_count() or 1
+
+    def efs(self, X, LAT, atmn, ND, urep=0.0, p_gpa=0.0, NM=512, XT=1):
+        X, LAT, atmn = Oracle._prep(X, LAT, atmn)
+        N = len(atmn)
+        F = np.zeros(3 * N)
+        S = np.zeros(6)
+        EA = np.zeros(N)
+        E = ctypes.c_double()
+        H = self.lib().ref_efs(self.dir, N, NM, ND, self.np, XT, _ip(atmn), _dp(LAT), _dp(X), urep, p_gpa,
+                               _dp(F), _dp(S), _dp(EA), ctypes.byref(E))
+        Xw = np.zeros(3 * N)
+        self.lib().ref_positions(N, _dp(Xw))
+        return dict(E=E.value, H=H, EA=EA, F=F.reshape(N, 3), U=S, X=Xw.reshape(N, 3))
+
+    def energy(self, X, LAT, atmn, ND, urep=0.0, p_gpa=0.0, NM=512):
+        X, LAT, atmn = Oracle._prep(X, LAT, atmn)
+        return self.lib().ref_energy(self.dir, len(atmn), NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), urep, p_gpa)
+
+    def descriptors(self, X, LAT, atmn, ND, NM=512, D=None):
+        X, LAT, atmn = Oracle._prep(X, LAT, atmn)
+        N = len(atmn)
+        G = np.zeros(N * 4096)
+        D = self.lib().ref_descriptors(self.dir, N, NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), _dp(G))
+        return G[: N * D].reshape(N, D)
+
+    def fn(self, atom, D, NM=512):
+        dnn = ctypes.c_int()
+        dni = np.zeros(NM + 1, np.int32)
+        Fn = np.zeros((NM + 1) * D * 3)
+        Sn = np.zeros(D * 6)
+        self.lib().ref_fn(atom, ctypes.byref(dnn), _ip(dni), _dp(Fn), _dp(Sn))
+        k = dnn.value
+        return dni[:k].copy(), Fn[: (k + 1) * D * 3].reshape(k + 1, D, 3), Sn.reshape(D, 6)
+
+    def relax(self, X, LAT, atmn, ND, rlxt=3, mitr=100, etol=1e-6, urep=0.0, p_gpa=0.0, NM=512):
+        X, LAT, atmn = Oracle._prep(X, LAT, atmn)
+        LAT = LAT.copy()
+        counts = np.zeros(3, np.int64)
+        H = self.lib().ref_relax(self.dir, len(atmn), NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), urep, p_gpa,
+                                 rlxt, mitr, etol, counts.ctypes.data_as(_L))
+        return dict(H=H, X=X.reshape(-1, 3), LAT=LAT.reshape(3, 3), n_energy=int(counts[0]),
+                    n_force=int(counts[1]), iters=int(counts[2]))
+
+    def nvt(self, X, LAT, atmn, ND, T, dt, tau, nsteps, seed=1, V=None, urep=0.0, NM=512):
+        X, LAT, atmn = Oracle._prep(X, LAT, atmn)
+        N = len(atmn)
+        vin = V is not None
+        V = np.ascontiguousarray(np.asarray(V, np.float64).reshape(-1)).copy() if vin else np.zeros(3 * N)
+        Hs = np.zeros(nsteps)
+        Ks = np.zeros(nsteps)
+        xi = self.lib().ref_nvt(self.dir, N, NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), _dp(V), int(vin),
+                                seed, T, dt, tau, nsteps, urep, _dp(Hs), _dp(Ks))
+        return dict(X=X.reshape(N, 3), V=V.reshape(N, 3), H=Hs, K=Ks, xi=xi)
+
+    def maxwell(self, X, LAT, atmn, ND, T, seed=1, NM=512):
+        X, LAT, atmn = Oracle._prep(X, LAT, atmn)
+        N = len(atmn)
+        V = np.zeros(3 * N)
+        self.lib().ref_maxwell(self.dir, N, NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), seed, T, _dp(V))
+        return V.reshape(N, 3)
+
+    def sizes(self):
+        out = (ctypes.c_int * 10)()
+        self.lib().ref_sizes(out)
+        return list(out)

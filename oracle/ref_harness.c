@@ -1,0 +1,287 @@
+/*
+ * ref_harness.c -- entry points into the reference MAISE sources compiled as
+ * a CPU oracle (oracle/_ref/libmaise_ref.so).  TEST INFRASTRUCTURE ONLY: used
+ * by tests/ to validate the C restatement (oracle/oracle.c) and the CUDA
+ * path, and by bench.py as the reference CPU baseline.
+ *
+ * Every evaluation goes through the reference's own code: the first call of
+ * a model runs CALL_MAISE (src/cmod.c:1164-1224), which reads ./model and
+ * allocates the reference structures; later calls reuse them.  Relaxation
+ * runs CELL_MIN (src/cmin.c:177-301) over the GSL stand-in of ref_shim.c.
+ * The NVT loop restates the integrator of Dynamics (src/cmod.c:385-453)
+ * around the reference CELL_FRC/CELL_KIN, because Dynamics itself writes
+ * files every step and overflows its Lindemann arrays for N > NM
+ * (src/cell.c:14-15, src/cmod.c:33-53).
+ */
+#include <omp.h>
+#include <stddef.h>
+#include <unistd.h>
+
+#include "mlib.h"
+
+extern long ECNTC, FCNTC; /* src/cmin.c:9 */
+
+static ANN hR;
+static PRS hP;
+static PRS hW[9];
+static LNK hL;
+static Cell hC;
+static int h_ready = 0, h_capN = 0, h_capNM = 0;
+static char h_dir[1024];
+
+/* CALL_MAISE in the model directory; (re)initialises when the model
+ * directory changes or the structure outgrows the first call's arrays. */
+static double h_call(const char *dir, int N, int NM, int ND, int NP, int XT, int *ATMN, double *LAT, double *X,
+                     double *FRC, double *STR, double urep, double p_gpa) {
+    char cwd[1024];
+    double H;
+    int reinit = !h_ready || N > h_capN || NM != h_capNM || strcmp(dir, h_dir) != 0;
+    if (reinit) {
+        /* arrays of a previous model are leaked on purpose: the reference never frees them */
+        memset(&hR, 0, sizeof(hR));
+        memset(&hP, 0, sizeof(hP));
+        memset(hW, 0, sizeof(hW));
+        memset(&hL, 0, sizeof(hL));
+        memset(&hC, 0, sizeof(hC));
+        hL.B = 0;
+        if (!getcwd(cwd, sizeof(cwd))) return NAN;
+        if (chdir(dir)) return NAN;
+    }
+    hR.UREP = urep;
+    hC.p = p_gpa;
+    H = CALL_MAISE(&hR, &hP, hW, &hL, &hC, 0, N, NM, ND, NP, XT, ATMN, LAT, X, FRC, STR);
+    if (reinit) {
+        if (chdir(cwd)) return NAN;
+        h_ready = 1;
+        h_capN = N;
+        h_capNM = NM;
+        snprintf(h_dir, sizeof(h_dir), "%s", dir);
+    }
+    return H;
+}
+
+/* the per-call field setup of CALL_MAISE (src/cmod.c:1170-1181) */
+static void h_prologue(int N, int NM, int ND, int NP, double p_gpa, double urep) {
+    hC.N = N;
+    hC.NM = NM;
+    hC.ND = ND;
+    hC.NP = NP;
+    hC.XT = 1;
+    hC.R0 = 1.0;
+    hR.JOBT = hC.JOBT = 20;
+    hR.NB = hC.NB = 1;
+    hR.A = hC.A = N;
+    hR.NP = NP;
+    hC.p = p_gpa / eV2GPa;
+    hR.UREP = urep;
+}
+
+int ref_sizes(int *out) {
+    out[0] = (int)sizeof(ANN);
+    out[1] = (int)sizeof(PRS);
+    out[2] = (int)sizeof(LNK);
+    out[3] = (int)sizeof(Cell);
+    out[4] = (int)offsetof(ANN, UREP);
+    out[5] = (int)offsetof(LNK, B);
+    out[6] = (int)offsetof(Cell, p);
+    out[7] = (int)offsetof(Cell, E);
+    out[8] = (int)offsetof(Cell, H);
+    out[9] = (int)offsetof(Cell, N);
+    return 10;
+}
+
+/* Energy, forces (FRC[3N]) and virial (STR[6]) through CALL_MAISE.
+ * EA (per-atom energies) and E_out (energy without pV) may be NULL. */
+double ref_efs(const char *dir, int N, int NM, int ND, int NP, int XT, int *ATMN, double *LAT, double *X, double urep,
+               double p_gpa, double *FRC, double *STR, double *EA, double *E_out) {
+    double H = h_call(dir, N, NM, ND, NP, XT, ATMN, LAT, X, FRC, STR, urep, p_gpa);
+    int i;
+    if (EA)
+        for (i = 0; i < N; i++) EA[i] = hC.EA[i];
+    if (E_out) *E_out = hC.E;
+    return H;
+}
+
+/* Energy only (CELL_ENE, src/cmod.c:128-151) on Cartesian X. */
+double ref_energy(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *LAT, double *X, double urep,
+                  double p_gpa) {
+    double *F = (double *)malloc(sizeof(double) * 3 * N), S[6];
+    double *Xc = (double *)malloc(sizeof(double) * 3 * N), H;
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    if (!h_ready || strcmp(dir, h_dir) != 0 || N > h_capN || NM != h_capNM)
+        h_call(dir, N, NM, ND, NP, 1, ATMN, LAT, Xc, F, S, urep, p_gpa);
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    h_prologue(N, NM, ND, NP, p_gpa, urep);
+    CAST_CELL(&hC, ATMN, LAT, Xc);
+    H = CELL_ENE(&hR, &hP, hW, &hC, &hL);
+    free(F);
+    free(Xc);
+    return H;
+}
+
+/* Descriptors G[N*D] via PARS_STR/PRS_BP with all derivative blocks
+ * computed (EFS = 3); ref_fn then reads one atom's blocks. */
+int ref_descriptors(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *LAT, double *X, double *G) {
+    double *F = (double *)malloc(sizeof(double) * 3 * N), S[6];
+    double *Xc = (double *)malloc(sizeof(double) * 3 * N);
+    int i, n;
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    if (!h_ready || strcmp(dir, h_dir) != 0 || N > h_capN || NM != h_capNM)
+        h_call(dir, N, NM, ND, NP, 1, ATMN, LAT, Xc, F, S, 0.0, 0.0);
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    h_prologue(N, NM, ND, NP, 0.0, 0.0);
+    CAST_CELL(&hC, ATMN, LAT, Xc);
+    for (i = 0; i < N; i++) hL.MRK[i] = 1;
+    hP.EFS = 3;
+    PARS_STR(&hP, hW, &hC, &hL, 0, ".");
+    for (i = 0; i < N; i++)
+        for (n = 0; n < hP.D; n++) G[(size_t)i * hP.D + n] = hL.Cn[i][n];
+    free(F);
+    free(Xc);
+    return hP.D;
+}
+
+/* Derivative blocks of one atom from the last ref_descriptors call, in the
+ * parse-file layout: fn[(slot*D+m)*3+q], slot == dnn is the self block. */
+int ref_fn(int atom, int *dnn, int *dni, double *fn, double *sn) {
+    int j, m, q, D = hP.D;
+    *dnn = hL.DNn[atom];
+    for (j = 0; j <= *dnn; j++) {
+        if (j < *dnn) dni[j] = hL.DNi[atom][j];
+        for (m = 0; m < D; m++)
+            for (q = 0; q < 3; q++) fn[((size_t)j * D + m) * 3 + q] = hL.Fn[atom][j][m][q];
+    }
+    if (sn)
+        for (m = 0; m < D; m++)
+            for (q = 0; q < 6; q++) sn[(size_t)m * 6 + q] = hL.Sn[atom][m][q];
+    return 0;
+}
+
+/* Wrapped Cartesian positions after the last evaluation (LIST wraps, src/cell.c:90-91). */
+int ref_positions(int N, double *X) {
+    int i, q;
+    for (i = 0; i < N; i++)
+        for (q = 0; q < 3; q++) X[3 * i + q] = hC.X[i][q];
+    return 0;
+}
+
+/* Cell relaxation through CELL_MIN (src/cmin.c:177-301).  On return X and
+ * LAT hold the relaxed Cartesian positions and lattice; counts[0..2] =
+ * energy calls, force calls, iterations. */
+double ref_relax(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *LAT, double *X, double urep,
+                 double p_gpa, int rlxt, int mitr, double etol, long *counts) {
+    double *F = (double *)malloc(sizeof(double) * 3 * N), S[6];
+    double *Xc = (double *)malloc(sizeof(double) * 3 * N), H;
+    int i, q, nfree = 0;
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    if (!h_ready || strcmp(dir, h_dir) != 0 || N > h_capN || NM != h_capNM)
+        h_call(dir, N, NM, ND, NP, 1, ATMN, LAT, Xc, F, S, urep, p_gpa);
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    h_prologue(N, NM, ND, NP, p_gpa, urep);
+    CAST_CELL(&hC, ATMN, LAT, Xc);
+    for (i = 0; i < N; i++)
+        for (q = 0; q < 3; q++) hC.FF[i][q] = 1;
+    hC.RLXT = rlxt;
+    hR.MINT = 0;
+    hC.MINT = 0;
+    hR.MITR = mitr;
+    hR.ETOL = etol;
+    hR.FRAC = 0.0;
+    hC.OUT = 0;
+    hC.it = 0;
+    JAR(&hC);
+    CELL_FRC(&hR, &hP, hW, &hC, &hL);
+    CELL_MIN(&hR, &hP, hW, &hC, &hL);
+    H = hC.H;
+    for (i = 0; i < N; i++)
+        for (q = 0; q < 3; q++) X[3 * i + q] = hC.X[i][q];
+    for (i = 0; i < 3; i++)
+        for (q = 0; q < 3; q++) LAT[3 * i + q] = hC.L[i][q];
+    counts[0] = ECNTC;
+    counts[1] = FCNTC;
+    counts[2] = hC.it;
+    (void)nfree;
+    free(F);
+    free(Xc);
+    return H;
+}
+
+/* NVT molecular dynamics: Maxwell initial velocities (src/cmod.c:224-280,
+ * Park-Miller streams src/util.c:1829-1873 seeded by PlantSeeds(seed)),
+ * then nsteps of the NVT branch of Dynamics (src/cmod.c:385-453):
+ *   E+F+S, K, xi += dt/tau^2 (2K/(3 N T) - 1), x += v dt + f dt^2/2,
+ *   v += f dt with f = F/m - xi v, wrap.
+ * If V is non-NULL and vin != 0 the given velocities are used instead of
+ * Maxwell's.  Hs[n], Ks[n] record H and K at the start of step n.  On
+ * return X and V hold the final state.  Returns the final xi. */
+double ref_nvt(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *LAT, double *X, double *V, int vin,
+               long seed, double T0, double dt, double tau, int nsteps, double urep, double *Hs, double *Ks) {
+    double *F = (double *)malloc(sizeof(double) * 3 * N), S[6];
+    double *Xc = (double *)malloc(sizeof(double) * 3 * N);
+    const double kbinv = 11604.0; /* src/cmod.c:5 */
+    double T = T0 / kbinv, xi = 0.0;
+    int i, q, n;
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    if (!h_ready || strcmp(dir, h_dir) != 0 || N > h_capN || NM != h_capNM)
+        h_call(dir, N, NM, ND, NP, 1, ATMN, LAT, Xc, F, S, urep, 0.0);
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    h_prologue(N, NM, ND, NP, 0.0, urep);
+    CAST_CELL(&hC, ATMN, LAT, Xc);
+    for (i = 0; i < N; i++)
+        for (q = 0; q < 3; q++) hC.FF[i][q] = 1;
+    if (vin && V) {
+        for (i = 0; i < N; i++)
+            for (q = 0; q < 3; q++) hC.V[i][q] = V[3 * i + q];
+    } else {
+        PlantSeeds(seed);
+        Maxwell(&hC, T, 20);
+    }
+    if (ND > 0) JAR(&hC);
+    for (n = 0; n < nsteps; n++) {
+        double fs;
+        hC.H = CELL_FRC(&hR, &hP, hW, &hC, &hL);
+        hC.K = CELL_KIN(&hC);
+        if (Hs) Hs[n] = hC.H;
+        if (Ks) Ks[n] = hC.K;
+        fs = 1.0 / (tau * tau) * (2.0 * hC.K / ((3.0 * (double)hC.N) * T) - 1.0);
+        xi += dt * fs;
+        for (i = 0; i < N; i++)
+            for (q = 0; q < 3; q++) {
+                double fi = hC.F[i][q] / hC.m[hC.ATMZ[i]] - xi * hC.V[i][q];
+                hC.X[i][q] += hC.V[i][q] * dt + 0.5 * fi * dt * dt;
+                hC.V[i][q] += fi * dt;
+            }
+        JAR(&hC);
+    }
+    for (i = 0; i < N; i++)
+        for (q = 0; q < 3; q++) {
+            X[3 * i + q] = hC.X[i][q];
+            if (V) V[3 * i + q] = hC.V[i][q];
+        }
+    free(F);
+    free(Xc);
+    return xi;
+}
+
+/* Maxwell velocities only (for seeding the GPU integrator identically). */
+int ref_maxwell(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *LAT, double *X, long seed, double T0,
+                double *V) {
+    double *F = (double *)malloc(sizeof(double) * 3 * N), S[6];
+    double *Xc = (double *)malloc(sizeof(double) * 3 * N);
+    int i, q;
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    if (!h_ready || strcmp(dir, h_dir) != 0 || N > h_capN || NM != h_capNM)
+        h_call(dir, N, NM, ND, NP, 1, ATMN, LAT, Xc, F, S, 0.0, 0.0);
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    h_prologue(N, NM, ND, NP, 0.0, 0.0);
+    CAST_CELL(&hC, ATMN, LAT, Xc);
+    for (i = 0; i < N; i++)
+        for (q = 0; q < 3; q++) hC.FF[i][q] = 1;
+    PlantSeeds(seed);
+    Maxwell(&hC, T0 / 11604.0, 20);
+    for (i = 0; i < N; i++)
+        for (q = 0; q < 3; q++) V[3 * i + q] = hC.V[i][q];
+    free(F);
+    free(Xc);
+    return 0;
+}

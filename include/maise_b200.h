@@ -1,0 +1,157 @@
+/*
+ * maise_b200.h -- C-ABI of the B200 implementation of MAISE's neural-network
+ * interatomic potential: Behler-Parrinello G2/G4 descriptors, per-species MLP
+ * energy with back-propagation to forces and virial, and the relaxation and
+ * NVT molecular-dynamics drivers that consume them.
+ *
+ * All entry points take plain pointers and sizes.  Host arrays are row-major:
+ *   x[3N]     positions (Cartesian unless stated; Angstrom)
+ *   lat9[9]   lattice vectors as rows, lat9[3*i+q] = component q of vector i
+ *   atmn[N]   species index of each atom in model order (0..nspc-1)
+ *   frc[3N]   forces (eV/Angstrom)
+ *   str[6]    virial U (eV, not divided by volume), order xx,yy,zz,xy,yz,zx
+ * Units and conventions are those of the reference (src/cmod.c:1136-1163).
+ *
+ * Every function returns MB_OK (0) or an MB_ERR_* code; mb_last_error()
+ * returns the message of the last failure in the calling thread.  Handles
+ * are not thread-safe: use one per host thread.
+ */
+#ifndef MAISE_B200_H
+#define MAISE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    MB_OK = 0,
+    MB_ERR_ARG = 1,        /* invalid argument */
+    MB_ERR_MODEL = 2,      /* model/basis file missing or malformed */
+    MB_ERR_NEIGHBOURS = 3, /* an atom reached NM neighbours (src/cell.c:134-142) */
+    MB_ERR_CUDA = 4,       /* CUDA runtime error */
+    MB_ERR_CAPACITY = 5,   /* structure larger than the reserved capacity */
+    MB_ERR_NOGPU = 6,      /* no usable sm_100 device */
+    MB_ERR_STATE = 7       /* invalid positions (non-finite, or wrap did not terminate) */
+};
+
+typedef struct mb_potential mb_potential;
+
+/* Message of the last error in this thread ("" if none). */
+const char *mb_last_error(void);
+
+/* Load a MAISE 'model' file (header, input ranges, weights and the appended
+ * basis) onto CUDA device `device`.
+ * Replaces the first-call initialisation of CALL_MAISE: READ_MODEL
+ * (src/util.c:1233-1335), Build_ANN/READ_ANN (src/nutl.c:305-357, 502-633)
+ * and Build_PRS (src/nprs.c:75-257). */
+int mb_open(const char *model_path, int device, mb_potential **out);
+int mb_close(mb_potential *pot);
+
+/* Model facts: number of species, their atomic numbers (spcz[nspc]),
+ * descriptor length D and the neighbour-list cutoff (Angstrom). */
+int mb_model_info(const mb_potential *pot, int *nspc, int *spcz, int *D, double *rc);
+
+/* Reserve device storage for structures of up to max_atoms atoms and
+ * max_neighbours neighbours per atom.  Optional: calls grow it on demand.
+ * Replaces the sizing done by Build_Cell/Build_LNK (src/cell.c:6-78,
+ * src/nutl.c:359-392), without their N x NM x NM angle tables. */
+int mb_reserve(mb_potential *pot, int max_atoms, int max_neighbours);
+
+/* Energy, forces and virial of one structure (CELL_FRC, src/cmod.c:153-191).
+ *   NM     neighbour cap: an atom with NM neighbours is an error, as in LIST
+ *   ND     number of periodic lattice directions (0 cluster, 3 crystal)
+ *   XT     0: x is fractional, 1: Cartesian (src/cmod.c:1108-1117)
+ *   p_gpa  external pressure; H = E + p V when ND == 3
+ *   urep   short-range repulsion strength U (eV); 0 disables (src/cmod.c:61-126)
+ * Outputs (any may be NULL): H, E, frc[3N], str[6], ea[N] (MLP per-atom
+ * energies), x_wrapped[3N] (positions after the wrap into the cell that
+ * LIST performs, src/cell.c:90-91).  |F|,|U| < 1e-8 are zeroed as in the
+ * reference. */
+int mb_efs(mb_potential *pot, int N, int NM, int ND, int XT, const int *atmn, const double *lat9, const double *x,
+           double p_gpa, double urep, double *H, double *E, double *frc, double *str, double *ea, double *x_wrapped);
+
+/* Energy only (CELL_ENE, src/cmod.c:128-151): descriptors + MLP forward. */
+int mb_energy(mb_potential *pot, int N, int NM, int ND, int XT, const int *atmn, const double *lat9, const double *x,
+              double p_gpa, double urep, double *H, double *E, double *ea);
+
+/* Descriptor vectors G[N*D] in the reference's species-resolved layout
+ * (the energy part of PRS_BP, src/nprs.c:445-566; L->Cn). */
+int mb_descriptors(mb_potential *pot, int N, int NM, int ND, int XT, const int *atmn, const double *lat9,
+                   const double *x, double *G);
+
+/* Vector-Jacobian product of the descriptor map with caller weights
+ * g[N*D]:  frc[i] = -sum_j sum_m g[j][m] dG_j,m/dx_i  and
+ * str = -sum_i sum_m g[i][m] dG_i,m/d(strain), i.e. the contraction
+ * FRC_ANN performs on Fn/Sn (src/nmlp.c:433-479) with dE/dG replaced by g.
+ * No noise zeroing is applied. */
+int mb_descriptor_vjp(mb_potential *pot, int N, int NM, int ND, int XT, const int *atmn, const double *lat9,
+                      const double *x, const double *g, double *frc, double *str);
+
+/* Cell relaxation (CELL_RELX/CELL_MIN, src/cmod.c:901-977,
+ * src/cmin.c:22-301).  Degrees of freedom as STR_BUF: fractional atom
+ * coordinates (rlxt 2), plus the 9 lattice components (rlxt 3), or the
+ * lattice only (rlxt 7).  BFGS with Fletcher's line search (step 0.01,
+ * tolerance 0.001); stops when |H - H_prev| < etol or after mitr
+ * iterations.  lat9 and x (Cartesian) are updated in place.
+ * counts (may be NULL) receives {energy calls, force calls, iterations}. */
+int mb_relax(mb_potential *pot, int N, int NM, int ND, const int *atmn, double *lat9, double *x, double p_gpa,
+             double urep, int rlxt, int mitr, double etol, double *H, long *counts);
+
+/* NVT molecular dynamics with the reference's thermostat (the RUNT == 2
+ * branch of Dynamics, src/cmod.c:403-407, 440-453), entirely on the GPU:
+ * per step  E+F+S -> K -> xi += dt/tau^2 (2K/(3 N T) - 1)
+ *           -> x += v dt + f dt^2/2, v += f dt  (f = F/m - xi v) -> wrap.
+ * v[3N] holds initial velocities (A/fs) and is updated; x (Cartesian) too.
+ * T in K, dt in fs, tau = coupling time CPLT in fs.  If Hs/Ks are non-NULL
+ * they receive H and K (eV) at the start of every step.  *xi carries the
+ * thermostat variable in and out. */
+int mb_md_nvt(mb_potential *pot, int N, int NM, int ND, const int *atmn, const double *lat9, double *x, double *v,
+              double T, double dt, double tau, int nsteps, double urep, double *xi, double *Hs, double *Ks);
+
+/* Maxwell initial velocities exactly as the reference draws them
+ * (src/cmod.c:224-280) from its Park-Miller generator seeded by
+ * PlantSeeds(seed) (src/util.c:1829-1873).  amu[N] are the atoms' masses
+ * in atomic mass units; v[3N] receives velocities in Angstrom/fs for
+ * temperature T (K).  Needs no GPU. */
+int mb_maxwell(int N, const double *amu, double T, long seed, double *v);
+
+/* Atomic mass (amu) of element z as tabulated by the reference (src/util.c:11). */
+double mb_atomic_mass(int z);
+
+/* ---- diagnostics (no counterpart in the reference) ---- */
+
+/* Start (enable=1) or stop timing of the fused descriptor/force kernel: every
+ * launch is bracketed by CUDA events on the handle's stream (up to
+ * `capacity` launches), and the kernel's pair/triplet counters are reset. */
+int mb_profile(mb_potential *pot, int enable, int capacity);
+
+/* Synchronise and report: summed duration (ms) and number of timed launches
+ * of the fused kernel, and the neighbour pairs and accepted triplets it
+ * processed since mb_profile(pot, 1, ...). */
+int mb_profile_read(mb_potential *pot, double *total_ms, int *launches, unsigned long long *pairs,
+                    unsigned long long *triplets);
+
+/* Time every step of mb_md_nvt with CUDA events (up to `capacity` steps)
+ * and, if flush_bytes > 0, overwrite a scratch buffer of that size between
+ * steps, outside the timed events, so that no step starts with the previous
+ * step's data in L2.  enable = 0 turns both off. */
+int mb_md_profile(mb_potential *pot, int enable, int capacity, size_t flush_bytes);
+
+/* Summed step time (ms) and number of timed steps since mb_md_profile(pot, 1, ...). */
+int mb_md_profile_read(mb_potential *pot, double *total_ms, int *steps);
+
+/* Sustained FP64 FMA throughput of `device` in TFLOP/s, measured with an
+ * FMA-chain kernel over every SM (a roofline denominator for FP64 work). */
+int mb_fp64_peak(int device, double *tflops);
+
+/* CUDA stream the handle launches on (a cudaStream_t), for callers that
+ * time or order work around it. */
+void *mb_stream(mb_potential *pot);
+
+/* Number of kernel launches this handle has issued since it was opened. */
+long mb_launch_count(const mb_potential *pot);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

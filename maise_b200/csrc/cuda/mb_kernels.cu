@@ -1,0 +1,994 @@
+/*
+ * mb_kernels.cu -- sm_100a kernels of libmaise_b200 (FP64 one-structure path).
+ *
+ *   k_wrap          wrap positions into the cell (JAR, src/cell.c:445-508)
+ *   k_nlist_brute   all (atom, image) pairs within Rc (LIST, src/cell.c:82-185)
+ *   k_cell_*        integer cell-list build (bin, count, scan, fill) and
+ *   k_nlist_cell    the same neighbour set from the 27 adjacent cells
+ *   k_efs           one CTA per central atom: G2/G4 descriptors
+ *                   (src/nprs.c:500-566), MLP forward and dE/dG
+ *                   (src/nmlp.c:367-431), then the reverse pass that turns
+ *                   dE_i/dG_i into forces on i and its neighbours and the
+ *                   virial (src/nprs.c:567-770 contracted as in
+ *                   src/nmlp.c:433-479) without materialising dG/dx
+ *   k_finalize      energy and virial reductions in fixed order, noise
+ *                   zeroing and enthalpy (src/cmod.c:153-191)
+ *   k_nvt_*         NVT thermostat and integrator (src/cmod.c:403-453)
+ *
+ * The wrap and the neighbour test use explicitly rounded operations
+ * (__dadd_rn/__dmul_rn, never contracted into FMAs) in the reference's
+ * operation order, so the selected neighbour set is the reference's.
+ */
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "../mb_internal.h"
+
+#define FULL 0xffffffffu
+
+namespace {
+
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+
+/* ------------------------------------------------------------------ */
+/* wrap                                                                */
+/* ------------------------------------------------------------------ */
+
+__global__ void k_wrap(int N, double *__restrict__ X, mb_cell c, int *status) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double x[3];
+    for (int q = 0; q < 3; q++) {
+        double s = 0.0;
+        for (int j = 0; j < 3; j++) s = xadd(s, xmul(X[3 * i + j], c.R[3 * q + j]));
+        x[q] = s;
+    }
+    for (int q = 0; q < 3; q++) {
+        int it = 0;
+        while (x[q] < 0.0 && it < 4096) { x[q] = xadd(x[q], 1.0); it++; }
+        while (x[q] >= 1.0 && it < 4096) { x[q] = xsub(x[q], 1.0); it++; }
+        if (!(x[q] >= 0.0 && x[q] < 1.0)) atomicOr(status, MB_ST_WRAP);
+    }
+    for (int q = 0; q < 3; q++) {
+        double s = 0.0;
+        for (int j = 0; j < 3; j++) s = xadd(s, xmul(x[j], c.L[3 * j + q]));
+        X[3 * i + q] = s;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* neighbour list                                                      */
+/* ------------------------------------------------------------------ */
+
+/* displacement of atom j's image (i0,i1,i2) from atom i and its squared
+ * length, formed exactly as src/cell.c:115-121 */
+__device__ __forceinline__ double image_disp(const mb_cell &c, const double *xi, const double *xj, int i0, int i1,
+                                             int i2, double *d) {
+    double r = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        double x = 0.0;
+        x = xadd(x, xmul((double)i0, c.L[q]));
+        x = xadd(x, xmul((double)i1, c.L[3 + q]));
+        x = xadd(x, xmul((double)i2, c.L[6 + q]));
+        x = xadd(x, xsub(xj[q], xi[q]));
+        d[q] = x;
+        r = xadd(r, xmul(x, x));
+    }
+    return r;
+}
+
+/* one warp per atom; candidates in the reference's order (j, then images) */
+__global__ void k_nlist_brute(int N, int NM, int cap, const double *__restrict__ X, mb_cell c, double rc2,
+                              int *__restrict__ nn, int *__restrict__ nj, double4 *__restrict__ nd, int *status) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= N) return;
+    int i = warp;
+    int w0 = 2 * c.Nq[0] + 1, w1 = 2 * c.Nq[1] + 1, w2 = 2 * c.Nq[2] + 1;
+    int nimg = w0 * w1 * w2;
+    long long total = (long long)N * nimg;
+    double xi[3] = {X[3 * i], X[3 * i + 1], X[3 * i + 2]};
+    int count = 0;
+    for (long long base = 0; base < total; base += 32) {
+        long long cidx = base + lane;
+        bool ok = false;
+        int j = 0;
+        double d[3] = {0, 0, 0}, r2 = 0.0;
+        if (cidx < total) {
+            j = (int)(cidx / nimg);
+            int im = (int)(cidx % nimg);
+            int i2 = im % w2 - c.Nq[2];
+            int t = im / w2;
+            int i1 = t % w1 - c.Nq[1];
+            int i0 = t / w1 - c.Nq[0];
+            if (!(j == i && i0 == 0 && i1 == 0 && i2 == 0)) {
+                double xj[3] = {X[3 * j], X[3 * j + 1], X[3 * j + 2]};
+                r2 = image_disp(c, xi, xj, i0, i1, i2, d);
+                ok = r2 < rc2;
+            }
+        }
+        unsigned m = __ballot_sync(FULL, ok);
+        int pos = count + __popc(m & ((1u << lane) - 1u));
+        if (ok && pos < cap) {
+            nj[(size_t)i * cap + pos] = j;
+            nd[(size_t)i * cap + pos] = make_double4(d[0], d[1], d[2], sqrt(r2));
+        }
+        count += __popc(m);
+    }
+    if (lane == 0) {
+        nn[i] = count < cap ? count : cap;
+        if (count >= NM) atomicOr(status, MB_ST_NBR_OVERFLOW);
+        if (count > cap) atomicOr(status, MB_ST_CAP_OVERFLOW);
+        atomicMax(&status[1], count);
+    }
+}
+
+__device__ __forceinline__ int cell_index(const mb_cell &c, const double *x, int *cq) {
+    for (int q = 0; q < 3; q++) {
+        double f = x[0] * c.R[3 * q] + x[1] * c.R[3 * q + 1] + x[2] * c.R[3 * q + 2];
+        int k = (int)floor(f * c.M[q]);
+        k = k < 0 ? 0 : (k >= c.M[q] ? c.M[q] - 1 : k);
+        cq[q] = k;
+    }
+    return (cq[0] * c.M[1] + cq[1]) * c.M[2] + cq[2];
+}
+
+__global__ void k_cell_bin(int N, const double *__restrict__ X, mb_cell c, int *cell_of, int *cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int cq[3];
+    int k = cell_index(c, X + 3 * i, cq);
+    cell_of[i] = k;
+    atomicAdd(&cnt[k], 1);
+}
+
+/* exclusive scan of the cell counts by one CTA; start[ncell] = N */
+__global__ void k_cell_scan(int ncell, const int *cnt, int *start) {
+    __shared__ int part[1024];
+    int t = threadIdx.x, nt = blockDim.x;
+    int per = (ncell + nt - 1) / nt, lo = t * per, hi = min(lo + per, ncell), s = 0;
+    for (int k = lo; k < hi; k++) s += cnt[k];
+    part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        int acc = 0;
+        for (int k = 0; k < nt; k++) {
+            int v = part[k];
+            part[k] = acc;
+            acc += v;
+        }
+    }
+    __syncthreads();
+    s = part[t];
+    for (int k = lo; k < hi; k++) {
+        start[k] = s;
+        s += cnt[k];
+    }
+    if (t == nt - 1) start[ncell] = s;
+}
+
+__global__ void k_cell_fill(int N, const int *cell_of, const int *start, int *cursor, int *atoms) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int k = cell_of[i];
+    int pos = atomicAdd(&cursor[k], 1);
+    atoms[start[k] + pos] = i;
+}
+
+/* order each cell's atoms by index so the neighbour order is deterministic */
+__global__ void k_cell_sort(int ncell, const int *start, int *atoms) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ncell) return;
+    int lo = start[k], hi = start[k + 1];
+    for (int a = lo + 1; a < hi; a++) {
+        int v = atoms[a], b = a - 1;
+        while (b >= lo && atoms[b] > v) {
+            atoms[b + 1] = atoms[b];
+            b--;
+        }
+        atoms[b + 1] = v;
+    }
+}
+
+/* One warp per atom over the 27 adjacent cells.  Periodic directions have
+ * at least 3 bins no thinner than Rc, so every image within Rc lies in an
+ * adjacent bin and each (atom, image) pair is visited once; the exact test
+ * then selects the reference's set. */
+__global__ void k_nlist_cell(int N, int NM, int cap, const double *__restrict__ X, mb_cell c, double rc2,
+                             const int *__restrict__ cell_of, const int *__restrict__ start,
+                             const int *__restrict__ atoms, int *__restrict__ nn, int *__restrict__ nj,
+                             double4 *__restrict__ nd, int *status) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= N) return;
+    int i = warp;
+    double xi[3] = {X[3 * i], X[3 * i + 1], X[3 * i + 2]};
+    int ci = cell_of[i];
+    int cq[3] = {ci / (c.M[1] * c.M[2]), (ci / c.M[2]) % c.M[1], ci % c.M[2]};
+    int count = 0;
+    for (int a = -1; a <= 1; a++)
+        for (int b = -1; b <= 1; b++)
+            for (int e = -1; e <= 1; e++) {
+                int dd[3] = {a, b, e}, cc[3], img[3];
+                bool skip = false;
+                for (int q = 0; q < 3; q++) {
+                    int k = cq[q] + dd[q];
+                    img[q] = 0;
+                    if (q < c.ND) {
+                        if (k < 0) { k += c.M[q]; img[q] = -1; }
+                        else if (k >= c.M[q]) { k -= c.M[q]; img[q] = 1; }
+                    } else if (k < 0 || k >= c.M[q]) {
+                        skip = true;
+                    }
+                    cc[q] = k;
+                }
+                if (skip) continue;
+                int cell = (cc[0] * c.M[1] + cc[1]) * c.M[2] + cc[2];
+                int lo = start[cell], hi = start[cell + 1];
+                for (int base = lo; base < hi; base += 32) {
+                    int idx = base + lane;
+                    bool ok = false;
+                    int j = 0;
+                    double d[3] = {0, 0, 0}, r2 = 0.0;
+                    if (idx < hi) {
+                        j = atoms[idx];
+                        if (!(j == i && img[0] == 0 && img[1] == 0 && img[2] == 0)) {
+                            double xj[3] = {X[3 * j], X[3 * j + 1], X[3 * j + 2]};
+                            r2 = image_disp(c, xi, xj, img[0], img[1], img[2], d);
+                            ok = r2 < rc2;
+                        }
+                    }
+                    unsigned m = __ballot_sync(FULL, ok);
+                    int pos = count + __popc(m & ((1u << lane) - 1u));
+                    if (ok && pos < cap) {
+                        nj[(size_t)i * cap + pos] = j;
+                        nd[(size_t)i * cap + pos] = make_double4(d[0], d[1], d[2], sqrt(r2));
+                    }
+                    count += __popc(m);
+                }
+            }
+    if (lane == 0) {
+        nn[i] = count < cap ? count : cap;
+        if (count >= NM) atomicOr(status, MB_ST_NBR_OVERFLOW);
+        if (count > cap) atomicOr(status, MB_ST_CAP_OVERFLOW);
+        atomicMax(&status[1], count);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* descriptor / MLP / force kernel                                     */
+/* ------------------------------------------------------------------ */
+
+__device__ __forceinline__ double fcut(double rc, double r) { return r > rc ? 0.0 : 0.5 * (cospi(r / rc) + 1.0); }
+
+__device__ __forceinline__ void fcut_d(double rc, double r, double &f, double &df) {
+    if (r > rc) {
+        f = 0.0;
+        df = 0.0;
+        return;
+    }
+    double s, co;
+    sincospi(r / rc, &s, &co);
+    f = 0.5 * (co + 1.0);
+    df = -0.5 * CUDART_PI / rc * s;
+}
+
+/* (1 + lambda c)^zeta * 2^(1-zeta) for every (zeta, lambda), and optionally
+ * the derivative in c; integer zeta by repeated squaring.  NZ and NLAM are
+ * upper bounds (exact for the specialised kernels); zl = z*NLAM + l. */
+template <int NZ, int NLAM>
+__device__ __forceinline__ void angular(const mb_params &P, double c, double *lz, double *lzp) {
+#pragma unroll
+    for (int l = 0; l < NLAM; l++) {
+        if (l >= P.nlam) break;
+        double lam = P.lam[l];
+        double base = 1.0 + lam * c;
+        if (P.zeta_int) {
+            double sq[7];
+            sq[0] = base;
+#pragma unroll
+            for (int k = 1; k < 7; k++) sq[k] = sq[k - 1] * sq[k - 1];
+#pragma unroll
+            for (int z = 0; z < NZ; z++) {
+                if (z >= P.nz) break;
+                int zb = P.zbits[z], mb = P.zm1bits[z];
+                double pw = 1.0, pm = 1.0;
+#pragma unroll
+                for (int k = 0; k < 7; k++) {
+                    if (zb & (1 << k)) pw *= sq[k];
+                    if (mb & (1 << k)) pm *= sq[k];
+                }
+                lz[z * NLAM + l] = P.powz[z] * pw;
+                if (lzp) lzp[z * NLAM + l] = P.powz[z] * P.zeta[z] * lam * pm;
+            }
+        } else {
+#pragma unroll
+            for (int z = 0; z < NZ; z++) {
+                if (z >= P.nz) break;
+                lz[z * NLAM + l] = P.powz[z] * pow(base, P.zeta[z]);
+                if (lzp) lzp[z * NLAM + l] = P.powz[z] * P.zeta[z] * lam * pow(base, P.zeta[z] - 1.0);
+            }
+        }
+    }
+}
+
+struct EfsArgs {
+    int N, cap, mode;
+    double urep;
+    const int *nn, *nj;
+    const double4 *nd;
+    const int *spc;
+    const mb_params *params;
+    const double *weights;
+    double *EA, *EU, *G, *F, *vir;
+    unsigned long long *counters; /* [0] pairs, [1] accepted forward triplets */
+};
+
+/* shared-memory carve-up of k_efs */
+struct EfsSmem {
+    int *j, *sp, *raw_sp;
+    double4 *d;
+    double *fa, *fb, *P, *Fnb, *G, *grid, *red, *tmp, *h;
+    unsigned *queue;
+    int *seg;  /* [0..3] counts, [4..7] offsets */
+};
+
+__host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7; }
+
+__host__ __device__ inline size_t efs_smem_bytes(int cap, int D, int ne, int ng2, int nzl_cells, int warps) {
+    size_t b = 0;
+    b += align8(sizeof(int) * cap) * 3;           /* j, sp, raw_sp */
+    b += sizeof(double4) * cap;                   /* d */
+    b += sizeof(double) * cap * 2;                /* fa, fb */
+    b += sizeof(double) * cap * ne;               /* P */
+    b += sizeof(double) * cap * 3;                /* Fnb */
+    b += sizeof(double) * D;                      /* G */
+    b += sizeof(double) * nzl_cells;              /* grid */
+    b += sizeof(double) * warps * 64;             /* red */
+    b += sizeof(double) * cap * (ng2 > 1 ? ng2 : 1); /* tmp */
+    b += sizeof(double) * 4 * MB_MAXH;            /* h */
+    b += sizeof(unsigned) * warps * 64;           /* queue */
+    b += sizeof(int) * 8;
+    return b;
+}
+
+__device__ inline EfsSmem efs_carve(char *base, int cap, int D, int ne, int ng2, int nzl_cells, int warps) {
+    EfsSmem s;
+    char *p = base;
+    s.d = (double4 *)p; p += sizeof(double4) * cap;
+    s.fa = (double *)p; p += sizeof(double) * cap;
+    s.fb = (double *)p; p += sizeof(double) * cap;
+    s.P = (double *)p; p += sizeof(double) * cap * ne;
+    s.Fnb = (double *)p; p += sizeof(double) * cap * 3;
+    s.G = (double *)p; p += sizeof(double) * D;
+    s.grid = (double *)p; p += sizeof(double) * nzl_cells;
+    s.red = (double *)p; p += sizeof(double) * warps * 64;
+    s.tmp = (double *)p; p += sizeof(double) * cap * (ng2 > 1 ? ng2 : 1);
+    s.h = (double *)p; p += sizeof(double) * 4 * MB_MAXH;
+    s.j = (int *)p; p += align8(sizeof(int) * cap);
+    s.sp = (int *)p; p += align8(sizeof(int) * cap);
+    s.raw_sp = (int *)p; p += align8(sizeof(int) * cap);
+    s.queue = (unsigned *)p; p += sizeof(unsigned) * warps * 64;
+    s.seg = (int *)p;
+    return s;
+}
+
+/* Sum of 64 per-lane values across a warp: afterwards lane l holds the
+ * sums of values 2l and 2l+1 (recursive halving). */
+__device__ __forceinline__ void warp_reduce64(double *v, int lane) {
+#pragma unroll
+    for (int step = 0; step < 5; step++) {
+        const int off = 16 >> step, half = 32 >> step;
+        const bool upper = (lane & off) != 0;
+#pragma unroll
+        for (int k = 0; k < half; k++) {
+            double send = upper ? v[k] : v[k + half];
+            double keep = upper ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(FULL, send, off);
+        }
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+/* CTA-wide reduction of a 64-cell accumulator grid into s.red[0..63]
+ * (warp 0 adds the warps' partial sums in a fixed order). */
+template <int WARPS>
+__device__ __forceinline__ void cta_reduce64(double *v, EfsSmem &s, int warp, int lane) {
+    warp_reduce64(v, lane);
+    s.red[warp * 64 + 2 * lane] = v[0];
+    s.red[warp * 64 + 2 * lane + 1] = v[1];
+    __syncthreads();
+    if (warp == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < WARPS; w++) {
+            a += s.red[w * 64 + 2 * lane];
+            b += s.red[w * 64 + 2 * lane + 1];
+        }
+        __syncwarp();
+        s.red[2 * lane] = a;
+        s.red[2 * lane + 1] = b;
+    }
+    __syncthreads();
+}
+
+/* Triplet candidates of block (a,b): rectangle seg_a x seg_b, j<k when a==b.
+ * Each warp compacts its accepted (j,k) pairs into a queue and processes
+ * them 32 at a time with all lanes active. */
+template <int WARPS, class Accept, class Body>
+__device__ __forceinline__ int for_triplets(EfsSmem &s, int a, int b, int warp, int lane, Accept accept, Body body) {
+    int accepted = 0;
+    int na = s.seg[a], nb = s.seg[b], oa = s.seg[4 + a], ob = s.seg[4 + b];
+    int total = na * nb;
+    unsigned *q = s.queue + warp * 64;
+    int qn = 0;
+    for (int base = warp * 32; base < total; base += WARPS * 32) {
+        int idx = base + lane;
+        bool ok = false;
+        unsigned pk = 0;
+        if (idx < total) {
+            int jj = oa + idx / nb, kk = ob + idx % nb;
+            if (a != b || jj < kk) {
+                ok = accept(jj, kk);
+                pk = (unsigned)jj | ((unsigned)kk << 16);
+            }
+        }
+        unsigned m = __ballot_sync(FULL, ok);
+        int pos = qn + __popc(m & ((1u << lane) - 1u));
+        if (ok) q[pos] = pk;
+        qn += __popc(m);
+        accepted += __popc(m);
+        __syncwarp();
+        if (qn >= 32) {
+            unsigned mine = q[lane];
+            __syncwarp();
+            if (lane < qn - 32) q[lane] = q[32 + lane];
+            qn -= 32;
+            __syncwarp();
+            body((int)(mine & 0xffffu), (int)(mine >> 16), true);
+        }
+    }
+    if (qn > 0) {
+        bool act = lane < qn;
+        unsigned mine = act ? q[lane] : 0u;
+        __syncwarp();
+        body((int)(mine & 0xffffu), (int)(mine >> 16), act);
+    }
+    return accepted;
+}
+
+template <int NE, int NZ, int NLAM, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
+    constexpr int NZL = NZ * NLAM;
+    extern __shared__ __align__(16) char smem_raw[];
+    const mb_params &P = *A.params;
+    const int i = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NT = WARPS * 32;
+    const int D = P.D, ns = P.nspc, ng2 = P.ng2, ne = P.ne, nzl = P.nzl;
+    EfsSmem s = efs_carve(smem_raw, A.cap, D, NE, ng2, NE * NZL, WARPS);
+    const int n = A.nn[i];
+    const int s0 = A.spc[i];
+    const double *net = A.weights + P.w_off[s0];
+
+    /* ---- stage neighbours, stably sorted by species relative to s0 ---- */
+    for (int t = tid; t < n; t += NT) s.raw_sp[t] = A.spc[A.nj[(size_t)i * A.cap + t]];
+    if (tid < 8) s.seg[tid] = 0;
+    for (int t = tid; t < D; t += NT) s.G[t] = 0.0;
+    __syncthreads();
+    if (tid == 0) {
+        int cnt[4] = {0, 0, 0, 0};
+        for (int t = 0; t < n; t++) cnt[(s.raw_sp[t] - s0 + ns) % ns]++;
+        int off = 0;
+        for (int v = 0; v < 4; v++) {
+            s.seg[v] = cnt[v];
+            s.seg[4 + v] = off;
+            off += cnt[v];
+        }
+    }
+    __syncthreads();
+    for (int t = tid; t < n; t += NT) {
+        int ds = (s.raw_sp[t] - s0 + ns) % ns, rank = 0;
+        for (int u = 0; u < t; u++) rank += ((s.raw_sp[u] - s0 + ns) % ns) == ds;
+        int dst = s.seg[4 + ds] + rank;
+        s.j[dst] = A.nj[(size_t)i * A.cap + t];
+        s.sp[dst] = s.raw_sp[t];
+        s.d[dst] = A.nd[(size_t)i * A.cap + t];
+    }
+    __syncthreads();
+
+    constexpr int CELLS = ((NE * NZL + 63) / 64) * 64;
+    if (A.mode != MB_MODE_VJP) {
+    /* ---- forward pair terms: fc, exponential factors, G2, repulsion ---- */
+    for (int t = tid; t < n; t += NT) {
+        double r = s.d[t].w;
+        int sj = s.sp[t], p = s0 * s0 + sj * sj;
+        double fa = fcut(P.f_rc2[p], r);
+        s.fa[t] = fa;
+        s.fb[t] = fcut(P.f_rc4[p], r);
+#pragma unroll
+        for (int e = 0; e < NE; e++)
+            if (e < ne) s.P[t * NE + e] = exp(-P.f_eta4[p][e] * r * r);
+        bool gate = r < P.f_rc2[p];
+        for (int f = 0; f < ng2; f++) {
+            double x = r - P.f_rs[p][f];
+            s.tmp[t * ng2 + f] = gate ? fa * exp(-P.f_eta2[p][f] * (x * x)) : 0.0;
+        }
+    }
+    __syncthreads();
+    /* G2 sums per relative species in neighbour order (deterministic) */
+    for (int w = tid; w < ns * ng2; w += NT) {
+        int v = w / ng2, f = w % ng2;
+        double acc = 0.0;
+        for (int t = s.seg[4 + v]; t < s.seg[4 + v] + s.seg[v]; t++) acc += s.tmp[t * ng2 + f];
+        s.G[P.ind2[v] + f] = acc;
+    }
+    if (A.urep > 0.0 && tid == 0) {
+        double eu = 0.0;
+        for (int t = 0; t < n; t++) {
+            double r = s.d[t].w, R = P.rm[s0] + P.rm[s.sp[t]];
+            if (r < R) eu += A.urep * fcut(R, r) * R / r;
+        }
+        A.EU[i] = eu;
+    }
+
+    /* ---- forward triplet terms, block by block of (species j, species k) ---- */
+    for (int a = 0; a < ns; a++)
+        for (int b = a; b < ns; b++) {
+            double acc[CELLS];
+#pragma unroll
+            for (int k = 0; k < CELLS; k++) acc[k] = 0.0;
+            auto accept = [&](int jj, int kk) -> bool {
+                double4 d1 = s.d[jj], d2 = s.d[kk];
+                int sj = s.sp[jj], sk = s.sp[kk];
+                int p01 = s0 * s0 + sj * sj, p02 = s0 * s0 + sk * sk, p12 = sj * sj + sk * sk;
+                double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+                double r3 = sqrt(dx * dx + dy * dy + dz * dz);
+                return d1.w < P.f_rc2[p01] && d1.w < P.f_rc4[p01] && d2.w < P.f_rc4[p02] && r3 < P.f_rc4[p12];
+            };
+            auto body = [&](int jj, int kk, bool act) {
+                if (!act) return;
+                double4 d1 = s.d[jj], d2 = s.d[kk];
+                int sj = s.sp[jj], sk = s.sp[kk], p12 = sj * sj + sk * sk;
+                double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+                double r3s = dx * dx + dy * dy + dz * dz, r3 = sqrt(r3s);
+                double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) / (d1.w * d2.w);
+                double A3 = 2.0 * s.fa[jj] * s.fb[kk] * fcut(P.f_rc4[p12], r3);
+                double lz[NZL];
+#pragma unroll
+                for (int k = 0; k < NZL; k++) lz[k] = 0.0;
+                angular<NZ, NLAM>(P, c, lz, nullptr);
+#pragma unroll
+                for (int e = 0; e < NE; e++) {
+                    if (e >= ne) break;
+                    double ex = A3 * s.P[jj * NE + e] * s.P[kk * NE + e] * exp(-P.f_eta4[p12][e] * r3s);
+#pragma unroll
+                    for (int zl = 0; zl < NZL; zl++)
+                        acc[e * NZL + zl] += ex * lz[zl];
+                }
+            };
+            int acc_t = for_triplets<WARPS>(s, a, b, warp, lane, accept, body);
+            if (lane == 0 && A.counters) atomicAdd(&A.counters[1], (unsigned long long)acc_t);
+            __syncthreads();
+#pragma unroll
+            for (int ch = 0; ch < CELLS / 64; ch++) {
+                cta_reduce64<WARPS>(acc + 64 * ch, s, warp, lane);
+                if (tid == 0) {
+                    int ds = a * a + b * b, base = P.ind4[ds];
+                    for (int f = 0; f < P.ng4; f++) {
+                        int cell = P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam;
+                        if (cell / 64 == ch) s.G[base + f] += s.red[cell % 64];
+                    }
+                }
+                __syncthreads();
+            }
+        }
+
+    if (A.mode == MB_MODE_DESCRIPTORS) {
+        for (int t = tid; t < D; t += NT) A.G[(size_t)i * D + t] = s.G[t];
+        return;
+    }
+    } /* end of the forward part (skipped for MB_MODE_VJP) */
+
+    /* ---- MLP: forward (src/nmlp.c:367-431) and dE/dG ---- */
+    const int h1 = P.h1, h2 = P.h2;
+    const double *off = net, *W0 = off + D, *b0 = W0 + h1 * D, *W1 = b0 + h1, *b1 = W1 + h2 * h1, *W2 = b1 + h2,
+                 *b2 = W2 + h2;
+    double *H1 = s.h, *H2 = s.h + MB_MAXH, *Dl1 = s.h + 2 * MB_MAXH, *Dl2 = s.h + 3 * MB_MAXH;
+    if (A.mode != MB_MODE_VJP) {
+        for (int m = warp; m < h1; m += WARPS) {
+            double acc = 0.0;
+            for (int l = lane; l < D; l += 32) acc += (s.G[l] - off[l]) * W0[m * D + l];
+            acc = warp_sum(acc);
+            if (lane == 0) H1[m] = tanh(b0[m] + acc);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double v = 0.0;
+            if (lane < h2) {
+                v = b1[lane];
+                for (int k = 0; k < h1; k++) v += H1[k] * W1[lane * h1 + k];
+                v = tanh(v);
+                H2[lane] = v;
+            }
+            double e = lane < h2 ? v * W2[lane] : 0.0;
+            e = warp_sum(e);
+            if (lane == 0) A.EA[i] = b2[0] + e;
+            __syncwarp();
+            if (lane < h2) Dl2[lane] = W2[lane] * (1.0 - v * v);
+            __syncwarp();
+            if (lane < h1) {
+                double g = 0.0;
+                for (int m = 0; m < h2; m++) g += Dl2[m] * W1[m * h1 + lane];
+                Dl1[lane] = g * (1.0 - H1[lane] * H1[lane]);
+            }
+        }
+        __syncthreads();
+        if (A.mode == MB_MODE_ENERGY) return;
+        /* s.G <- dE_i/dG_i */
+        for (int l = tid; l < D; l += NT) {
+            double g = 0.0;
+            for (int k = 0; k < h1; k++) g += Dl1[k] * W0[k * D + l];
+            s.G[l] = g;
+        }
+    } else {
+        for (int l = tid; l < D; l += NT) s.G[l] = A.G[(size_t)i * D + l];
+    }
+    __syncthreads();
+
+    /* ---- reverse pair terms with the species-0 parameters ---- */
+    double fi[3] = {0.0, 0.0, 0.0}, vr[6] = {0, 0, 0, 0, 0, 0};
+    for (int t = tid; t < n; t += NT) {
+        double4 d = s.d[t];
+        double r = d.w, ir = 1.0 / r;
+        double f4, df4, f2, df2;
+        fcut_d(P.d_rc4, r, f4, df4);
+        fcut_d(P.d_rc2, r, f2, df2);
+        s.fa[t] = f4;
+        s.fb[t] = df4;
+#pragma unroll
+        for (int e = 0; e < NE; e++)
+            if (e < ne) s.P[t * NE + e] = exp(-P.d_eta4[e] * r * r);
+        int ds1 = (s.sp[t] - s0 + ns) % ns;
+        const double *g = s.G + P.ind2[ds1];
+        double cpair = 0.0;
+        for (int f = 0; f < ng2; f++) {
+            double x = r - P.d_rs[f], eta = P.d_eta2[f];
+            cpair += g[f] * exp(-eta * x * x) * (-2.0 * eta * x * f2 + df2);
+        }
+        /* dE/dd = cpair d / r : force +on i, -on j; virial -= (dE/dd) (x) d */
+        double cr = cpair * ir;
+        double v0 = cr * d.x, v1 = cr * d.y, v2 = cr * d.z;
+        fi[0] += v0; fi[1] += v1; fi[2] += v2;
+        s.Fnb[3 * t] = -v0; s.Fnb[3 * t + 1] = -v1; s.Fnb[3 * t + 2] = -v2;
+        vr[0] -= v0 * d.x; vr[1] -= v1 * d.y; vr[2] -= v2 * d.z;
+        vr[3] -= v0 * d.y; vr[4] -= v1 * d.z; vr[5] -= v2 * d.x;
+        if (A.urep > 0.0) {
+            double R = P.rm[s0] + P.rm[s.sp[t]];
+            if (r < R) {
+                /* CELL_UREP on the ordered pair (i, j): force on i only (src/cmod.c:100-112) */
+                double fu, dfu;
+                fcut_d(R, r, fu, dfu);
+                double tu = -2.0 * A.urep * R / (r * r) * (-fu / r + dfu);
+                fi[0] -= tu * d.x; fi[1] -= tu * d.y; fi[2] -= tu * d.z;
+                vr[0] += 0.5 * tu * d.x * d.x; vr[1] += 0.5 * tu * d.y * d.y; vr[2] += 0.5 * tu * d.z * d.z;
+                vr[3] += 0.5 * tu * d.x * d.y; vr[4] += 0.5 * tu * d.y * d.z; vr[5] += 0.5 * tu * d.z * d.x;
+            }
+        }
+    }
+    __syncthreads();
+
+    /* ---- reverse triplet terms ---- */
+    for (int a = 0; a < ns; a++)
+        for (int b = a; b < ns; b++) {
+            const int ds = a * a + b * b, base = P.ind4[ds];
+            for (int t = tid; t < NE * NZL; t += NT) s.grid[t] = 0.0;
+            __syncthreads();
+            if (tid == 0)
+                for (int f = 0; f < P.ng4; f++)
+                    s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam] += s.G[base + f];
+            __syncthreads();
+            auto accept = [&](int jj, int kk) -> bool {
+                double4 d1 = s.d[jj], d2 = s.d[kk];
+                double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+                double r3 = sqrt(dx * dx + dy * dy + dz * dz);
+                return d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3 < P.d_rc4;
+            };
+            auto body = [&](int jj, int kk, bool act) {
+                if (!act) return;
+                double4 d1 = s.d[jj], d2 = s.d[kk];
+                double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
+                double r3s = wx * wx + wy * wy + wz * wz, r3 = sqrt(r3s);
+                double r1 = d1.w, r2 = d2.w, ir1 = 1.0 / r1, ir2 = 1.0 / r2, ir3 = 1.0 / r3;
+                double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
+                double f3, df3;
+                fcut_d(P.d_rc4, r3, f3, df3);
+                double f1 = s.fa[jj], df1 = s.fb[jj], f2 = s.fa[kk], df2 = s.fb[kk];
+                double lz[NZL], lzp[NZL];
+#pragma unroll
+                for (int k = 0; k < NZL; k++) { lz[k] = 0.0; lzp[k] = 0.0; }
+                angular<NZ, NLAM>(P, c, lz, lzp);
+                double Q = 0.0, Qe = 0.0, Qc = 0.0;
+#pragma unroll
+                for (int e = 0; e < NE; e++) {
+                    if (e >= ne) break;
+                    double ex = s.P[jj * NE + e] * s.P[kk * NE + e] * exp(-P.d_eta4[e] * r3s);
+                    double u = 0.0, v = 0.0;
+#pragma unroll
+                    for (int zl = 0; zl < NZL; zl++) {
+                        double cg = s.grid[e * NZL + zl];
+                        u += cg * lz[zl];
+                        v += cg * lzp[zl];
+                    }
+                    Q += ex * u;
+                    Qe += P.d_eta4[e] * ex * u;
+                    Qc += ex * v;
+                }
+                double Af = 2.0 * f1 * f2 * f3;
+                double T1 = 2.0 * df1 * f2 * f3 * Q - 2.0 * r1 * Af * Qe;
+                double T2 = 2.0 * f1 * df2 * f3 * Q - 2.0 * r2 * Af * Qe;
+                double T3 = 2.0 * f1 * f2 * df3 * Q - 2.0 * r3 * Af * Qe;
+                double Tc = Af * Qc;
+                double a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
+                double a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
+                double g1x = a11 * d1.x + a12 * d2.x - a3 * wx, g1y = a11 * d1.y + a12 * d2.y - a3 * wy,
+                       g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
+                double g2x = a22 * d2.x + a12 * d1.x + a3 * wx, g2y = a22 * d2.y + a12 * d1.y + a3 * wy,
+                       g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                fi[0] += g1x + g2x; fi[1] += g1y + g2y; fi[2] += g1z + g2z;
+                atomicAdd(&s.Fnb[3 * jj], -g1x); atomicAdd(&s.Fnb[3 * jj + 1], -g1y); atomicAdd(&s.Fnb[3 * jj + 2], -g1z);
+                atomicAdd(&s.Fnb[3 * kk], -g2x); atomicAdd(&s.Fnb[3 * kk + 1], -g2y); atomicAdd(&s.Fnb[3 * kk + 2], -g2z);
+                vr[0] -= g1x * d1.x + g2x * d2.x;
+                vr[1] -= g1y * d1.y + g2y * d2.y;
+                vr[2] -= g1z * d1.z + g2z * d2.z;
+                vr[3] -= g1x * d1.y + g2x * d2.y;
+                vr[4] -= g1y * d1.z + g2y * d2.z;
+                vr[5] -= g1z * d1.x + g2z * d2.x;
+            };
+            for_triplets<WARPS>(s, a, b, warp, lane, accept, body);
+            __syncthreads();
+        }
+
+    /* ---- write forces and the virial of atom i ---- */
+    {
+        double v[64];
+#pragma unroll
+        for (int k = 0; k < 64; k++) v[k] = 0.0;
+        v[0] = fi[0]; v[1] = fi[1]; v[2] = fi[2];
+#pragma unroll
+        for (int k = 0; k < 6; k++) v[3 + k] = vr[k];
+        cta_reduce64<WARPS>(v, s, warp, lane);
+        if (tid == 0) {
+            atomicAdd(&A.F[3 * i], s.red[0]);
+            atomicAdd(&A.F[3 * i + 1], s.red[1]);
+            atomicAdd(&A.F[3 * i + 2], s.red[2]);
+            for (int k = 0; k < 6; k++) A.vir[(size_t)i * 6 + k] = s.red[3 + k];
+        }
+        for (int t = tid; t < n; t += NT) {
+            int j = s.j[t];
+            atomicAdd(&A.F[3 * j], s.Fnb[3 * t]);
+            atomicAdd(&A.F[3 * j + 1], s.Fnb[3 * t + 1]);
+            atomicAdd(&A.F[3 * j + 2], s.Fnb[3 * t + 2]);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* reductions                                                          */
+/* ------------------------------------------------------------------ */
+
+/* out[0]=E, out[1]=H, out[2..7]=U; fixed-order block reduction */
+__global__ void k_finalize(int N, int mode, double pV, const double *EA, const double *EU, const double *vir,
+                           double *F, double *out) {
+    __shared__ double red[7][256];
+    int t = threadIdx.x;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int i = t; i < N; i += 256) {
+        acc[0] += EA[i] + EU[i];
+        if (mode != MB_MODE_ENERGY)
+            for (int k = 0; k < 6; k++) acc[1 + k] += vir[(size_t)i * 6 + k];
+    }
+    for (int k = 0; k < 7; k++) red[k][t] = acc[k];
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (t < h)
+            for (int k = 0; k < 7; k++) red[k][t] += red[k][t + h];
+        __syncthreads();
+    }
+    if (t == 0) {
+        out[0] = red[0][0];
+        out[1] = red[0][0] + pV;
+        for (int k = 0; k < 6; k++) {
+            double u = red[1 + k][0];
+            if (mode == MB_MODE_EFS && fabs(u) < 1e-8) u = 0.0;
+            out[2 + k] = u;
+        }
+    }
+    if (mode == MB_MODE_EFS)
+        for (int i = t; i < 3 * N; i += 256)
+            if (fabs(F[i]) < 1e-8) F[i] = 0.0;
+}
+
+/* ------------------------------------------------------------------ */
+/* NVT step (src/cmod.c:403-407, 440-453)                              */
+/* ------------------------------------------------------------------ */
+
+/* K = 1/2 sum m v^2 in atom order, then xi += dt/tau^2 (2K/(3NT) - 1).
+ * out[8] = K, out[9] = xi; trace[2*step] = H, trace[2*step+1] = K. */
+__global__ void k_nvt_thermostat(int N, const double *V, const int *spc, const double *mass, double dt, double tau,
+                                 double T, int step, double *out, double *trace, int capTrace) {
+    __shared__ double red[256];
+    int t = threadIdx.x;
+    double k = 0.0;
+    for (int i = t; i < N; i += 256) {
+        double m = mass[spc[i]];
+        k += m * V[3 * i] * V[3 * i] + m * V[3 * i + 1] * V[3 * i + 1] + m * V[3 * i + 2] * V[3 * i + 2];
+    }
+    red[t] = k;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (t < h) red[t] += red[t + h];
+        __syncthreads();
+    }
+    if (t == 0) {
+        double K = 0.5 * red[0];
+        double fs = 1.0 / (tau * tau) * (2.0 * K / ((3.0 * (double)N) * T) - 1.0);
+        out[8] = K;
+        out[9] += dt * fs;
+        if (step >= 0 && step < capTrace) {
+            trace[2 * step] = out[1];
+            trace[2 * step + 1] = K;
+        }
+    }
+}
+
+__global__ void k_nvt_integrate(int N, double *X, double *V, const double *F, const int *spc, const double *mass,
+                                double dt, const double *out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double xi = out[9], m = mass[spc[i]];
+    for (int q = 0; q < 3; q++) {
+        double v = V[3 * i + q];
+        double f = F[3 * i + q] / m - xi * v;
+        X[3 * i + q] += v * dt + 0.5 * f * dt * dt;
+        V[3 * i + q] = v + f * dt;
+    }
+}
+
+__global__ void k_set_out(double *out, int idx, double v) { out[idx] = v; }
+
+} /* namespace */
+
+/* ------------------------------------------------------------------ */
+/* launchers                                                           */
+/* ------------------------------------------------------------------ */
+
+#define MB_EFS_WARPS 4
+
+/* specialised kernel for the reference bases: 7 G4 exponents, 4 zeta, 2 lambda */
+static bool efs_fast(const mb_model *m) { return m->P.ne <= 7 && m->P.nz <= 4 && m->P.nlam <= 2; }
+
+extern "C" size_t mbk_efs_smem(const mb_model *m, int capNB, int warps) {
+    bool fast = efs_fast(m);
+    int ne = fast ? 7 : MB_MAXE;
+    int cells = fast ? 7 * 8 : MB_MAXE * 8 * 4;
+    return efs_smem_bytes(capNB, m->P.D, ne, m->P.ng2, cells, warps);
+}
+
+extern "C" int mbk_wrap(mb_dev *d, int N, const mb_cell *c, void *stream, long *launches) {
+    if (c->ND <= 0 || N <= 0) return 0;
+    k_wrap<<<(N + 127) / 128, 128, 0, (cudaStream_t)stream>>>(N, d->X, *c, d->status);
+    (*launches)++;
+    return (int)cudaGetLastError();
+}
+
+extern "C" int mbk_nlist(mb_dev *d, int N, int NM, const mb_cell *c, double rc, void *stream, long *launches) {
+    cudaStream_t st = (cudaStream_t)stream;
+    double rc2 = rc * rc;
+    int warps_per_block = 4;
+    int blocks = (N + warps_per_block - 1) / warps_per_block;
+    if (c->M[0] > 0) {
+        int ncell = c->M[0] * c->M[1] * c->M[2];
+        cudaMemsetAsync(d->cell_cnt, 0, sizeof(int) * ncell, st);
+        k_cell_bin<<<(N + 127) / 128, 128, 0, st>>>(N, d->X, *c, d->cell_of, d->cell_cnt);
+        k_cell_scan<<<1, 1024, 0, st>>>(ncell, d->cell_cnt, d->cell_start);
+        cudaMemsetAsync(d->cell_cnt, 0, sizeof(int) * ncell, st);
+        k_cell_fill<<<(N + 127) / 128, 128, 0, st>>>(N, d->cell_of, d->cell_start, d->cell_cnt, d->cell_atoms);
+        k_cell_sort<<<(ncell + 127) / 128, 128, 0, st>>>(ncell, d->cell_start, d->cell_atoms);
+        k_nlist_cell<<<blocks, warps_per_block * 32, 0, st>>>(N, NM, d->capNB, d->X, *c, rc2, d->cell_of,
+                                                              d->cell_start, d->cell_atoms, d->nn, d->nj,
+                                                              (double4 *)d->nd, d->status);
+        *launches += 5;
+    } else {
+        k_nlist_brute<<<blocks, warps_per_block * 32, 0, st>>>(N, NM, d->capNB, d->X, *c, rc2, d->nn, d->nj,
+                                                               (double4 *)d->nd, d->status);
+        *launches += 1;
+    }
+    return (int)cudaGetLastError();
+}
+
+template <int NE, int NZ, int NLAM>
+static int launch_efs(const EfsArgs &a, size_t smem, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
+    auto kern = k_efs<NE, NZ, NLAM, MB_EFS_WARPS>;
+    static size_t configured = 0;
+    if (smem > 48 * 1024 && smem > configured) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        configured = smem;
+    }
+    if (e0) cudaEventRecord(e0, st);
+    kern<<<a.N, MB_EFS_WARPS * 32, smem, st>>>(a);
+    if (e1) cudaEventRecord(e1, st);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode, double urep, int need_nb_max,
+                                   int nb_max, void *stream, long *launches) {
+    (void)need_nb_max;
+    (void)nb_max;
+    cudaStream_t st = (cudaStream_t)stream;
+    EfsArgs a;
+    a.N = N;
+    a.cap = d->capNB;
+    a.mode = mode;
+    a.urep = urep;
+    a.nn = d->nn;
+    a.nj = d->nj;
+    a.nd = (const double4 *)d->nd;
+    a.spc = d->spc;
+    a.params = d->params;
+    a.weights = d->weights;
+    a.EA = d->EA;
+    a.EU = d->EU;
+    a.G = d->G;
+    a.F = d->F;
+    a.vir = d->vir;
+    a.counters = d->counters;
+    cudaEvent_t e0 = 0, e1 = 0;
+    if (d->ev_on && d->ev_n < d->ev_cap) {
+        e0 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n];
+        e1 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n + 1];
+        d->ev_n++;
+    }
+    cudaMemsetAsync(d->EU, 0, sizeof(double) * N, st);
+    if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
+    size_t smem = mbk_efs_smem(m, d->capNB, MB_EFS_WARPS);
+    int rc;
+    if (smem > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
+    if (efs_fast(m))
+        rc = launch_efs<7, 4, 2>(a, smem, st, e0, e1);
+    else if (m->P.nz <= 8 && m->P.nlam <= 4)
+        rc = launch_efs<MB_MAXE, 8, 4>(a, smem, st, e0, e1);
+    else
+        rc = (int)cudaErrorInvalidValue;
+    (*launches)++;
+    return rc;
+}
+
+extern "C" int mbk_finalize(mb_dev *d, int N, int mode, double pV, void *stream, long *launches) {
+    k_finalize<<<1, 256, 0, (cudaStream_t)stream>>>(N, mode, pV, d->EA, d->EU, d->vir, d->F, d->out);
+    (*launches)++;
+    return (int)cudaGetLastError();
+}
+
+extern "C" int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, int step,
+                              void *stream, long *launches) {
+    cudaStream_t st = (cudaStream_t)stream;
+    (void)m;
+    /* masses by species live after the weights in the parameter upload (see mb_core.c) */
+    const double *mass = d->weights + m->weights_len;
+    k_nvt_thermostat<<<1, 256, 0, st>>>(N, d->V, d->spc, mass, dt, tau, T, step, d->out, d->trace, d->capTrace);
+    k_nvt_integrate<<<(N + 127) / 128, 128, 0, st>>>(N, d->X, d->V, d->F, d->spc, mass, dt, d->out);
+    *launches += 2;
+    return (int)cudaGetLastError();
+}
+
+extern "C" int mbk_set_xi(mb_dev *d, double xi, void *stream) {
+    k_set_out<<<1, 1, 0, (cudaStream_t)stream>>>(d->out, 9, xi);
+    return (int)cudaGetLastError();
+}

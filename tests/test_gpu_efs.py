@@ -1,0 +1,255 @@
+"""GPU parity of the one-structure FP64 path (descriptors, forces, virial,
+energy) against the oracle and the reference's golden vectors, through the
+C-ABI.  Tolerances: 1e-10 relative energy, 1e-9 eV/A force (the plain-path
+requirement), descriptors to 1e-12 relative."""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_golden, parse_structures, write_model_dir
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+E_RTOL = 1e-10
+F_ATOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def mb():
+    import maise_b200
+
+    return maise_b200
+
+
+def test_descriptors_match_golden_parse_files(mb, parse_golden, parse_model_dir):
+    pot = mb.Potential(parse_model_dir + "/model")
+    worst = 0.0
+    for s, LAT, X, atmn, Gref in parse_structures(parse_golden):
+        G = pot.descriptors(X, LAT, atmn, ND=3, NM=400)
+        err = np.abs(G - Gref) / (1e-13 + 1e-12 * np.abs(Gref))
+        worst = max(worst, float(err.max()))
+    assert worst <= 1.0, worst
+
+
+def test_vjp_matches_golden_derivative_blocks(mb, parse_golden, parse_model_dir):
+    """Force on a marked atom for arbitrary weights g equals the contraction
+    of the reference's printed dG/dx blocks (src/nprs.c:419-431)."""
+    pot = mb.Potential(parse_model_dir + "/model")
+    off = parse_golden["offsets"]
+    rng = np.random.default_rng(0)
+    for k in range(len(parse_golden["mk_atom"])):
+        s, atom = int(parse_golden["mk_struct"][k]), int(parse_golden["mk_atom"][k])
+        a, b = off[s], off[s + 1]
+        X, at, L = parse_golden["x"][a:b], parse_golden["atmn"][a:b], parse_golden["lat"][s]
+        g = rng.normal(size=(len(at), 82))
+        F, _ = pot.descriptor_vjp(X, L, at, g, ND=3, NM=400)
+        dni, Fn = parse_golden["mk_dni"][k], parse_golden["mk_fn"][k]
+        owners = list(dni) + [atom]
+        want = -sum(Fn[slot].T @ g[o] for slot, o in enumerate(owners))
+        np.testing.assert_allclose(F[atom], want, rtol=1e-10, atol=1e-10)
+
+
+def test_vjp_matches_oracle_including_virial(mb, tmp_path):
+    c = load_golden("ref_efs.npz")["cases"][2]
+    d = write_model_dir(tmp_path, c["model"])
+    pot, o = mb.Potential(d + "/model"), Oracle(d + "/model")
+    g = np.random.default_rng(1).normal(size=(len(c["atmn"]), pot.D))
+    F, U = pot.descriptor_vjp(c["X"], c["LAT"], c["atmn"], g, ND=3, NM=400)
+    Fo, Uo = o.vjp(c["X"], c["LAT"], c["atmn"], 3, g, NM=400)
+    np.testing.assert_allclose(F, Fo, atol=1e-9)
+    np.testing.assert_allclose(U, Uo, rtol=1e-10, atol=1e-9)
+
+
+@pytest.mark.parametrize("case", range(5))
+def test_efs_matches_reference_vectors(mb, tmp_path, case):
+    c = load_golden("ref_efs.npz")["cases"][case]
+    d = write_model_dir(tmp_path, c["model"])
+    pot = mb.Potential(d + "/model")
+    r = pot.efs(c["X"], c["LAT"], c["atmn"], ND=int(c["ND"]), NM=400, urep=float(c["urep"]), p_gpa=float(c["p"]))
+    assert r["H"] == pytest.approx(float(c["H"]), rel=E_RTOL)
+    np.testing.assert_allclose(r["EA"], c["EA"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(r["F"], c["F"], atol=F_ATOL)
+    np.testing.assert_allclose(r["U"], c["U"], rtol=E_RTOL, atol=1e-9)
+    G = pot.descriptors(c["X"], c["LAT"], c["atmn"], ND=int(c["ND"]), NM=400)
+    np.testing.assert_allclose(G, c["G"], rtol=1e-12, atol=1e-13)
+    e = pot.energy(c["X"], c["LAT"], c["atmn"], ND=int(c["ND"]), NM=400, urep=float(c["urep"]), p_gpa=float(c["p"]))
+    assert e["H"] == pytest.approx(r["H"], rel=1e-14)
+
+
+def test_interface_known_answer_through_mb_efs(mb, tmp_path):
+    g = load_golden("kat_interface.npz")
+    d = write_model_dir(tmp_path, g["model"])
+    pot = mb.Potential(d + "/model")
+    r = pot.efs(g["X"], g["LAT"], g["atmn"], ND=0, NM=500)
+    assert r["H"] == pytest.approx(float(g["outcar_H"]), abs=5e-9)
+    assert r["H"] == pytest.approx(float(g["ref_H"]), rel=1e-12)
+    np.testing.assert_allclose(r["F"], g["ref_F"], atol=1e-10)
+    np.testing.assert_allclose(r["U"], g["ref_U"], rtol=1e-11, atol=1e-11)
+    np.testing.assert_allclose(r["EA"], float(g["outcar_EA"]), atol=5e-13)
+
+
+def test_call_maise_drop_in(mb, tmp_path):
+    """CALL_MAISE with caller-owned reference structs, run in a fresh process
+    inside the model directory as the reference's interface programs do."""
+    g = load_golden("kat_interface.npz")
+    d = write_model_dir(tmp_path, g["model"])
+    script = f"""
+import ctypes, numpy as np, sys
+sys.path.insert(0, {ROOT!r})
+import maise_b200 as mb
+lib = mb.load_library()
+R = ctypes.create_string_buffer(4704); P = ctypes.create_string_buffer(160)
+W = ctypes.create_string_buffer(160 * 9); L = ctypes.create_string_buffer(376); C = ctypes.create_string_buffer(10624)
+ctypes.c_double.from_buffer(R, 4688).value = 0.0
+ctypes.c_int.from_buffer(L, 152).value = 0
+D = ctypes.POINTER(ctypes.c_double)
+X = np.array([[2.0,0,0],[-2.0,0,0],[0,2.0,0],[0,-2.0,0]]).ravel().copy(); LAT = (np.eye(3)*20).ravel().copy()
+AT = np.zeros(4, np.int32); F = np.zeros(12); S = np.zeros(6)
+for k in range(2):
+    ctypes.c_double.from_buffer(C, 1736).value = 0.0
+    H = lib.CALL_MAISE(ctypes.addressof(R), ctypes.addressof(P), ctypes.addressof(W), ctypes.addressof(L),
+                       ctypes.addressof(C), 0, 4, 500, 0, 4, 1, AT.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                       LAT.ctypes.data_as(D), X.ctypes.data_as(D), F.ctypes.data_as(D), S.ctypes.data_as(D))
+    assert ctypes.c_int.from_buffer(L, 152).value == 1
+    assert ctypes.c_double.from_buffer(C, 1768).value == H
+print(repr(H), *map(repr, F), *map(repr, S))
+"""
+    out = subprocess.run([sys.executable, "-c", script], cwd=d, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    vals = [float(v) for v in out.stdout.split()]
+    assert vals[0] == pytest.approx(float(g["ref_H"]), rel=1e-12)
+    np.testing.assert_allclose(np.array(vals[1:13]).reshape(4, 3), g["ref_F"], atol=1e-10)
+    np.testing.assert_allclose(vals[13:19], g["ref_U"], rtol=1e-11, atol=1e-11)
+
+
+def _model_for(tmp_path, w, seed=2, name="m"):
+    from maise_b200 import models
+
+    d = tmp_path / name
+    d.mkdir(exist_ok=True)
+    models.random_model(str(d / "model"), w["spcz"], models.Basis(), (w["X"], w["LAT"], w["atmn"], w["ND"]),
+                        seed=seed)
+    return str(d)
+
+
+def test_cell_list_path_matches_oracle(mb, tmp_path):
+    """500-atom ternary alloy: 19 A cell takes the cell-list neighbour build."""
+    from maise_b200 import workloads
+
+    w = workloads.random_alloy(n=5, a=3.8, seed=3, jitter=0.1)
+    d = _model_for(tmp_path, w)
+    pot, o = mb.Potential(d + "/model"), Oracle(d + "/model")
+    r = pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=200)
+    ro = o.efs(w["X"], w["LAT"], w["atmn"], 3, NM=200)
+    assert r["H"] == pytest.approx(ro["H"], rel=E_RTOL)
+    np.testing.assert_allclose(r["F"], ro["F"], atol=F_ATOL)
+    np.testing.assert_allclose(r["U"], ro["U"], rtol=E_RTOL, atol=1e-8)
+    np.testing.assert_array_equal(r["X"], ro["X"])
+
+
+def test_neighbour_sets_equal_reference_list(mb, tmp_path):
+    """Per-atom neighbour counts of the GPU list equal LIST's (src/cell.c:82-185)
+    through the pair-count-sensitive G2 with eta -> 0 (sum of cutoff terms)."""
+    from maise_b200 import workloads
+
+    rng = np.random.default_rng(9)
+    X, L, at = workloads.random_cell(20, rng, 2)
+    w = dict(X=X, LAT=L, atmn=at, ND=3, spcz=[29, 47])
+    d = _model_for(tmp_path, w)
+    o = Oracle(d + "/model")
+    nn, *_ = o.nlist(X, L, at, 3, NM=400)
+    pot = mb.Potential(d + "/model")
+    G = pot.descriptors(X, L, at, ND=3, NM=400)
+    Go = o.descriptors(X, L, at, 3, NM=400)
+    np.testing.assert_allclose(G, Go, rtol=1e-12, atol=1e-13)
+    assert nn.min() > 10
+
+
+def test_energy_only_and_enthalpy(mb, tmp_path):
+    c = load_golden("ref_efs.npz")["cases"][1]
+    d = write_model_dir(tmp_path, c["model"])
+    pot = mb.Potential(d + "/model")
+    e0 = pot.energy(c["X"], c["LAT"], c["atmn"], ND=3, NM=400)
+    e1 = pot.energy(c["X"], c["LAT"], c["atmn"], ND=3, NM=400, p_gpa=10.0)
+    V = abs(np.linalg.det(c["LAT"]))
+    assert e1["H"] - e0["H"] == pytest.approx(10.0 / 160.2176565 * V, rel=1e-12)
+    assert e1["E"] == e0["E"]
+
+
+def test_fractional_input(mb, tmp_path):
+    c = load_golden("ref_efs.npz")["cases"][0]
+    d = write_model_dir(tmp_path, c["model"])
+    pot = mb.Potential(d + "/model")
+    xf = c["X"] @ np.linalg.inv(c["LAT"])
+    r0 = pot.efs(c["X"], c["LAT"], c["atmn"], ND=3, NM=400)
+    r1 = pot.efs(xf, c["LAT"], c["atmn"], ND=3, NM=400, XT=0)
+    assert r1["H"] == pytest.approx(r0["H"], rel=1e-12)
+    np.testing.assert_allclose(r1["F"], r0["F"], atol=1e-9)
+
+
+def test_neighbour_overflow_is_an_error(mb, tmp_path):
+    c = load_golden("ref_efs.npz")["cases"][0]
+    d = write_model_dir(tmp_path, c["model"])
+    pot = mb.Potential(d + "/model")
+    with pytest.raises(mb.MaiseError) as e:
+        pot.efs(c["X"], c["LAT"], c["atmn"], ND=3, NM=40)
+    assert e.value.code == 3
+    # the handle stays usable
+    r = pot.efs(c["X"], c["LAT"], c["atmn"], ND=3, NM=400)
+    assert np.isfinite(r["H"])
+
+
+def test_capacity_growth_between_calls(mb, tmp_path):
+    """Small then dense structure: neighbour capacity grows on demand."""
+    from maise_b200 import workloads
+
+    w = workloads.fcc_supercell(n=3, a=3.61, jitter=0.05, seed=5)
+    d = _model_for(tmp_path, w)
+    pot, o = mb.Potential(d + "/model"), Oracle(d + "/model")
+    pot.reserve(8, 8)
+    r = pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=300)
+    ro = o.efs(w["X"], w["LAT"], w["atmn"], 3, NM=300)
+    assert r["H"] == pytest.approx(ro["H"], rel=E_RTOL)
+    np.testing.assert_allclose(r["F"], ro["F"], atol=F_ATOL)
+
+
+def test_nonfinite_positions_are_rejected(mb, tmp_path):
+    c = load_golden("ref_efs.npz")["cases"][0]
+    d = write_model_dir(tmp_path, c["model"])
+    pot = mb.Potential(d + "/model")
+    X = np.array(c["X"], float)
+    X[3, 1] = np.nan
+    with pytest.raises(mb.MaiseError) as e:
+        pot.efs(X, c["LAT"], c["atmn"], ND=3, NM=400)
+    assert e.value.code == 7
+    assert np.isfinite(pot.efs(c["X"], c["LAT"], c["atmn"], ND=3, NM=400)["H"])
+
+
+def test_full_size_ternary_invariants(mb, tmp_path):
+    """4000-atom Cu-Pd-Ag: forces sum to zero, translation invariance, and
+    central differences on sampled atoms (size-independent properties)."""
+    from maise_b200 import workloads
+
+    w = workloads.random_alloy(n=10, a=3.8, seed=0, jitter=0.05)
+    d = _model_for(tmp_path, w)
+    pot = mb.Potential(d + "/model")
+    r = pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=200)
+    assert np.abs(r["F"].sum(0)).max() < 1e-9 * len(w["atmn"])
+    r2 = pot.efs(w["X"] + np.array([0.3, -0.2, 0.7]), w["LAT"], w["atmn"], ND=3, NM=200)
+    assert r2["E"] == pytest.approx(r["E"], rel=1e-12)
+    X = np.array(w["X"], float)
+    h = 1e-4
+    for i, q in [(7, 0), (1500, 1), (3999, 2)]:
+        Xp, Xm = X.copy(), X.copy()
+        Xp[i, q] += h
+        Xm[i, q] -= h
+        Ep = pot.energy(Xp, w["LAT"], w["atmn"], ND=3, NM=200)["E"]
+        Em = pot.energy(Xm, w["LAT"], w["atmn"], ND=3, NM=200)["E"]
+        assert -(Ep - Em) / (2 * h) == pytest.approx(r["F"][i, q], abs=1e-6)

@@ -324,24 +324,29 @@ struct EfsArgs {
     const double *weights;
     double *EA, *EU, *G, *F, *vir;
     unsigned long long *counters; /* [0] pairs, [1] accepted forward triplets */
+    size_t smem_group;            /* shared-memory bytes of one atom group */
+    int tl_cap;                   /* triplet-list entries of one atom group */
 };
 
-/* shared-memory carve-up of k_efs */
+/* shared-memory carve-up of one atom group of k_efs */
 struct EfsSmem {
     int *j, *sp, *raw_sp;
     double4 *d;
-    double *fa, *fb, *P, *Fnb, *G, *grid, *red, *tmp, *h;
-    unsigned *queue;
-    int *seg;  /* [0..3] counts, [4..7] offsets */
+    double *ir, *fa, *fb, *P, *Fnb, *G, *grid, *red, *tmp, *h;
+    unsigned *tl;  /* accepted (j,k) pairs: per-warp regions of tlw entries */
+    int *blk;      /* [block][warp][2] ranges of each warp's region per species block */
+    int *seg;      /* [0..3] counts, [4..7] offsets */
 };
+
+#define MB_MAX_BLOCKS 6 /* species blocks (a<=b) for 3 species */
 
 __host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7; }
 
-__host__ __device__ inline size_t efs_smem_bytes(int cap, int D, int ne, int ng2, int nzl_cells, int warps) {
+__host__ __device__ inline size_t efs_smem_bytes(int cap, int D, int ne, int ng2, int nzl_cells, int warps, int tl) {
     size_t b = 0;
     b += align8(sizeof(int) * cap) * 3;           /* j, sp, raw_sp */
     b += sizeof(double4) * cap;                   /* d */
-    b += sizeof(double) * cap * 2;                /* fa, fb */
+    b += sizeof(double) * cap * 3;                /* ir, fa, fb */
     b += sizeof(double) * cap * ne;               /* P */
     b += sizeof(double) * cap * 3;                /* Fnb */
     b += sizeof(double) * D;                      /* G */
@@ -349,15 +354,18 @@ __host__ __device__ inline size_t efs_smem_bytes(int cap, int D, int ne, int ng2
     b += sizeof(double) * warps * 64;             /* red */
     b += sizeof(double) * cap * (ng2 > 1 ? ng2 : 1); /* tmp */
     b += sizeof(double) * 4 * MB_MAXH;            /* h */
-    b += sizeof(unsigned) * warps * 64;           /* queue */
+    b += align8(sizeof(unsigned) * tl);           /* tl */
+    b += align8(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
     b += sizeof(int) * 8;
     return b;
 }
 
-__device__ inline EfsSmem efs_carve(char *base, int cap, int D, int ne, int ng2, int nzl_cells, int warps) {
+__device__ inline EfsSmem efs_carve(char *base, int cap, int D, int ne, int ng2, int nzl_cells, int warps, int tl) {
+    /* one atom group's region; `warps` = warps per atom */
     EfsSmem s;
     char *p = base;
     s.d = (double4 *)p; p += sizeof(double4) * cap;
+    s.ir = (double *)p; p += sizeof(double) * cap;
     s.fa = (double *)p; p += sizeof(double) * cap;
     s.fb = (double *)p; p += sizeof(double) * cap;
     s.P = (double *)p; p += sizeof(double) * cap * ne;
@@ -370,7 +378,8 @@ __device__ inline EfsSmem efs_carve(char *base, int cap, int D, int ne, int ng2,
     s.j = (int *)p; p += align8(sizeof(int) * cap);
     s.sp = (int *)p; p += align8(sizeof(int) * cap);
     s.raw_sp = (int *)p; p += align8(sizeof(int) * cap);
-    s.queue = (unsigned *)p; p += sizeof(unsigned) * warps * 64;
+    s.tl = (unsigned *)p; p += align8(sizeof(unsigned) * tl);
+    s.blk = (int *)p; p += align8(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
     s.seg = (int *)p;
     return s;
 }
@@ -397,17 +406,31 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-/* CTA-wide reduction of a 64-cell accumulator grid into s.red[0..63]
- * (warp 0 adds the warps' partial sums in a fixed order). */
-template <int WARPS>
-__device__ __forceinline__ void cta_reduce64(double *v, EfsSmem &s, int warp, int lane) {
+template <int WPA>
+__device__ __forceinline__ void group_sync() {
+    if (WPA == 1)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
+/* Reduction of a 64-cell accumulator grid over the atom's group into
+ * s.red[0..63] (warp 0 adds the warps' partial sums in a fixed order). */
+template <int WPA>
+__device__ __forceinline__ void group_reduce64(double *v, EfsSmem &s, int gwarp, int lane) {
     warp_reduce64(v, lane);
-    s.red[warp * 64 + 2 * lane] = v[0];
-    s.red[warp * 64 + 2 * lane + 1] = v[1];
+    if (WPA == 1) {
+        s.red[2 * lane] = v[0];
+        s.red[2 * lane + 1] = v[1];
+        __syncwarp();
+        return;
+    }
+    s.red[gwarp * 64 + 2 * lane] = v[0];
+    s.red[gwarp * 64 + 2 * lane + 1] = v[1];
     __syncthreads();
-    if (warp == 0) {
+    if (gwarp == 0) {
         double a = 0.0, b = 0.0;
-        for (int w = 0; w < WARPS; w++) {
+        for (int w = 0; w < WPA; w++) {
             a += s.red[w * 64 + 2 * lane];
             b += s.red[w * 64 + 2 * lane + 1];
         }
@@ -418,60 +441,79 @@ __device__ __forceinline__ void cta_reduce64(double *v, EfsSmem &s, int warp, in
     __syncthreads();
 }
 
-/* Triplet candidates of block (a,b): rectangle seg_a x seg_b, j<k when a==b.
- * Each warp compacts its accepted (j,k) pairs into a queue and processes
- * them 32 at a time with all lanes active. */
-template <int WARPS, class Accept, class Body>
-__device__ __forceinline__ int for_triplets(EfsSmem &s, int a, int b, int warp, int lane, Accept accept, Body body) {
-    int accepted = 0;
-    int na = s.seg[a], nb = s.seg[b], oa = s.seg[4 + a], ob = s.seg[4 + b];
-    int total = na * nb;
-    unsigned *q = s.queue + warp * 64;
-    int qn = 0;
-    for (int base = warp * 32; base < total; base += WARPS * 32) {
-        int idx = base + lane;
-        bool ok = false;
-        unsigned pk = 0;
-        if (idx < total) {
-            int jj = oa + idx / nb, kk = ob + idx % nb;
-            if (a != b || jj < kk) {
-                ok = accept(jj, kk);
-                pk = (unsigned)jj | ((unsigned)kk << 16);
-            }
-        }
-        unsigned m = __ballot_sync(FULL, ok);
-        int pos = qn + __popc(m & ((1u << lane) - 1u));
-        if (ok) q[pos] = pk;
-        qn += __popc(m);
-        accepted += __popc(m);
-        __syncwarp();
-        if (qn >= 32) {
-            unsigned mine = q[lane];
-            __syncwarp();
-            if (lane < qn - 32) q[lane] = q[32 + lane];
-            qn -= 32;
-            __syncwarp();
-            body((int)(mine & 0xffffu), (int)(mine >> 16), true);
+/* Triplet candidates of species block (a,b) are the pairs (j,k) of the
+ * rectangle seg_a x seg_b (j<k when a==b).  Rows j are dealt round-robin to
+ * the group's warps; each warp appends its accepted pairs to its own region
+ * [lo,hi) of the list, a row at a time, and stops before a row that might
+ * not fit.  Returns the next unprocessed row of this warp. */
+template <int WPA, class Accept>
+__device__ __forceinline__ int fill_rows(const EfsSmem &s, int a, int b, int row, int &pos, int hi, int lane,
+                                         Accept accept) {
+    const int na = s.seg[a], nb = s.seg[b], oa = s.seg[4 + a], ob = s.seg[4 + b];
+    for (; row < na; row += WPA) {
+        const int jj = oa + row, k0 = (a == b) ? row + 1 : 0;
+        if (pos + (nb - k0) > hi) break;
+        for (int kb = k0; kb < nb; kb += 32) {
+            const int kk = ob + kb + lane;
+            const bool ok = (kb + lane < nb) && accept(jj, kk);
+            const unsigned m = __ballot_sync(FULL, ok);
+            if (ok) s.tl[pos + __popc(m & ((1u << lane) - 1u))] = (unsigned)jj | ((unsigned)kk << 16);
+            pos += __popc(m);
         }
     }
-    if (qn > 0) {
-        bool act = lane < qn;
-        unsigned mine = act ? q[lane] : 0u;
-        __syncwarp();
-        body((int)(mine & 0xffffu), (int)(mine >> 16), act);
-    }
-    return accepted;
+    __syncwarp();
+    return row;
 }
 
-template <int NE, int NZ, int NLAM, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
+/* body(jj, kk) over list entries [from, to), one entry per lane */
+template <class Body>
+__device__ __forceinline__ void run_list(const EfsSmem &s, int from, int to, int lane, Body body) {
+    for (int t = from + lane; t < to; t += 32) {
+        const unsigned pk = s.tl[t];
+        body((int)(pk & 0xffffu), (int)(pk >> 16));
+    }
+}
+
+/* Enumerate block (a,b) for this warp and process it, reusing the list
+ * entries [blk[0], blk[1]) when `reuse` and filling (in rounds when the
+ * region overflows) otherwise.  Records the range for later reuse and
+ * returns 0 if the region overflowed (then the range is not reusable). */
+template <int WPA, class Accept, class Body>
+__device__ __forceinline__ int for_block(const EfsSmem &s, int a, int b, int *blk, int reuse, int &pos, int lo,
+                                         int hi, int warp, int lane, Accept accept, Body body) {
+    if (reuse) {
+        run_list(s, blk[0], blk[1], lane, body);
+        return 1;
+    }
+    int start = pos, row = warp, whole = 1;
+    for (;;) {
+        const int from = pos;
+        row = fill_rows<WPA>(s, a, b, row, pos, hi, lane, accept);
+        run_list(s, from, pos, lane, body);
+        __syncwarp();
+        if (row >= s.seg[a]) break;
+        whole = 0; /* region full: restart it for the next round */
+        start = pos = lo;
+    }
+    blk[0] = start;
+    blk[1] = pos;
+    return whole;
+}
+
+template <int NE, int NZ, int NLAM, int WPA, int APB>
+__global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
     constexpr int NZL = NZ * NLAM;
+    constexpr int WARPS = WPA;
     extern __shared__ __align__(16) char smem_raw[];
     const mb_params &P = *A.params;
-    const int i = blockIdx.x;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NT = WARPS * 32;
-    const int D = P.D, ns = P.nspc, ng2 = P.ng2, ne = P.ne, nzl = P.nzl;
-    EfsSmem s = efs_carve(smem_raw, A.cap, D, NE, ng2, NE * NZL, WARPS);
+    const int NT = WPA * 32, group = threadIdx.x / NT;
+    const int tid = threadIdx.x % NT, lane = threadIdx.x & 31, warp = tid >> 5;
+    const int i = blockIdx.x * APB + group;
+    if (i >= A.N) return; /* whole atom groups only: no barrier spans two groups */
+    const int D = P.D, ns = P.nspc, ng2 = P.ng2, ne = P.ne;
+    EfsSmem s = efs_carve(smem_raw + (size_t)group * A.smem_group, A.cap, D, NE, ng2, NE * NZL, WARPS, A.tl_cap);
+    const int tlw = A.tl_cap / WPA, tl_lo = warp * tlw, tl_hi = tl_lo + tlw;
+    int tl_pos = tl_lo, tl_whole = 1;
     const int n = A.nn[i];
     const int s0 = A.spc[i];
     const double *net = A.weights + P.w_off[s0];
@@ -480,7 +522,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
     for (int t = tid; t < n; t += NT) s.raw_sp[t] = A.spc[A.nj[(size_t)i * A.cap + t]];
     if (tid < 8) s.seg[tid] = 0;
     for (int t = tid; t < D; t += NT) s.G[t] = 0.0;
-    __syncthreads();
+    group_sync<WPA>();
     if (tid == 0) {
         int cnt[4] = {0, 0, 0, 0};
         for (int t = 0; t < n; t++) cnt[(s.raw_sp[t] - s0 + ns) % ns]++;
@@ -491,18 +533,33 @@ __global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
             off += cnt[v];
         }
     }
-    __syncthreads();
+    group_sync<WPA>();
     for (int t = tid; t < n; t += NT) {
         int ds = (s.raw_sp[t] - s0 + ns) % ns, rank = 0;
         for (int u = 0; u < t; u++) rank += ((s.raw_sp[u] - s0 + ns) % ns) == ds;
         int dst = s.seg[4 + ds] + rank;
         s.j[dst] = A.nj[(size_t)i * A.cap + t];
         s.sp[dst] = s.raw_sp[t];
-        s.d[dst] = A.nd[(size_t)i * A.cap + t];
+        double4 dv = A.nd[(size_t)i * A.cap + t];
+        s.d[dst] = dv;
+        s.ir[dst] = 1.0 / dv.w;
     }
-    __syncthreads();
+    group_sync<WPA>();
+    if (tid == 0 && A.counters) atomicAdd(&A.counters[0], (unsigned long long)n);
 
     constexpr int CELLS = ((NE * NZL + 63) / 64) * 64;
+    /* list gate: the union of the forward and derivative triplet gates
+     * (they coincide unless species blocks carry different cutoffs) */
+    auto accept_union = [&](int jj, int kk) -> bool {
+        double4 d1 = s.d[jj], d2 = s.d[kk];
+        int sj = s.sp[jj], sk = s.sp[kk];
+        int p01 = s0 * s0 + sj * sj, p02 = s0 * s0 + sk * sk, p12 = sj * sj + sk * sk;
+        double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+        double r3s = dx * dx + dy * dy + dz * dz;
+        bool fwd = d1.w < P.f_rc2[p01] && d1.w < P.f_rc4[p01] && d2.w < P.f_rc4[p02] && r3s < P.f_rc4sq[p12];
+        bool rev = d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq;
+        return fwd || rev;
+    };
     if (A.mode != MB_MODE_VJP) {
     /* ---- forward pair terms: fc, exponential factors, G2, repulsion ---- */
     for (int t = tid; t < n; t += NT) {
@@ -520,7 +577,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
             s.tmp[t * ng2 + f] = gate ? fa * exp(-P.f_eta2[p][f] * (x * x)) : 0.0;
         }
     }
-    __syncthreads();
+    group_sync<WPA>();
     /* G2 sums per relative species in neighbour order (deterministic) */
     for (int w = tid; w < ns * ng2; w += NT) {
         int v = w / ng2, f = w % ng2;
@@ -538,56 +595,59 @@ __global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
     }
 
     /* ---- forward triplet terms, block by block of (species j, species k) ---- */
-    for (int a = 0; a < ns; a++)
-        for (int b = a; b < ns; b++) {
-            double acc[CELLS];
+    {
+        int blkid = 0;
+        unsigned long long nacc = 0;
+        for (int a = 0; a < ns; a++)
+            for (int b = a; b < ns; b++, blkid++) {
+                double acc[CELLS];
 #pragma unroll
-            for (int k = 0; k < CELLS; k++) acc[k] = 0.0;
-            auto accept = [&](int jj, int kk) -> bool {
-                double4 d1 = s.d[jj], d2 = s.d[kk];
-                int sj = s.sp[jj], sk = s.sp[kk];
-                int p01 = s0 * s0 + sj * sj, p02 = s0 * s0 + sk * sk, p12 = sj * sj + sk * sk;
-                double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
-                double r3 = sqrt(dx * dx + dy * dy + dz * dz);
-                return d1.w < P.f_rc2[p01] && d1.w < P.f_rc4[p01] && d2.w < P.f_rc4[p02] && r3 < P.f_rc4[p12];
-            };
-            auto body = [&](int jj, int kk, bool act) {
-                if (!act) return;
-                double4 d1 = s.d[jj], d2 = s.d[kk];
-                int sj = s.sp[jj], sk = s.sp[kk], p12 = sj * sj + sk * sk;
-                double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
-                double r3s = dx * dx + dy * dy + dz * dz, r3 = sqrt(r3s);
-                double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) / (d1.w * d2.w);
-                double A3 = 2.0 * s.fa[jj] * s.fb[kk] * fcut(P.f_rc4[p12], r3);
-                double lz[NZL];
+                for (int k = 0; k < CELLS; k++) acc[k] = 0.0;
+                auto body = [&](int jj, int kk) {
+                    double4 d1 = s.d[jj], d2 = s.d[kk];
+                    int sj = s.sp[jj], sk = s.sp[kk];
+                    int p01 = s0 * s0 + sj * sj, p02 = s0 * s0 + sk * sk, p12 = sj * sj + sk * sk;
+                    double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+                    double r3s = dx * dx + dy * dy + dz * dz;
+                    if (!(d1.w < P.f_rc2[p01] && d1.w < P.f_rc4[p01] && d2.w < P.f_rc4[p02] && r3s < P.f_rc4sq[p12]))
+                        return;
+                    nacc++;
+                    double r3 = sqrt(r3s);
+                    double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (s.ir[jj] * s.ir[kk]);
+                    double A3 = 2.0 * s.fa[jj] * s.fb[kk] * fcut(P.f_rc4[p12], r3);
+                    double lz[NZL];
 #pragma unroll
-                for (int k = 0; k < NZL; k++) lz[k] = 0.0;
-                angular<NZ, NLAM>(P, c, lz, nullptr);
+                    for (int k = 0; k < NZL; k++) lz[k] = 0.0;
+                    angular<NZ, NLAM>(P, c, lz, nullptr);
 #pragma unroll
-                for (int e = 0; e < NE; e++) {
-                    if (e >= ne) break;
-                    double ex = A3 * s.P[jj * NE + e] * s.P[kk * NE + e] * exp(-P.f_eta4[p12][e] * r3s);
+                    for (int e = 0; e < NE; e++) {
+                        if (e >= ne) break;
+                        double ex = A3 * s.P[jj * NE + e] * s.P[kk * NE + e] * exp(-P.f_eta4[p12][e] * r3s);
 #pragma unroll
-                    for (int zl = 0; zl < NZL; zl++)
-                        acc[e * NZL + zl] += ex * lz[zl];
-                }
-            };
-            int acc_t = for_triplets<WARPS>(s, a, b, warp, lane, accept, body);
-            if (lane == 0 && A.counters) atomicAdd(&A.counters[1], (unsigned long long)acc_t);
-            __syncthreads();
-#pragma unroll
-            for (int ch = 0; ch < CELLS / 64; ch++) {
-                cta_reduce64<WARPS>(acc + 64 * ch, s, warp, lane);
-                if (tid == 0) {
-                    int ds = a * a + b * b, base = P.ind4[ds];
-                    for (int f = 0; f < P.ng4; f++) {
-                        int cell = P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam;
-                        if (cell / 64 == ch) s.G[base + f] += s.red[cell % 64];
+                        for (int zl = 0; zl < NZL; zl++) acc[e * NZL + zl] += ex * lz[zl];
                     }
+                };
+                int *blk = s.blk + (blkid * WPA + warp) * 2;
+                tl_whole &= for_block<WPA>(s, a, b, blk, 0, tl_pos, tl_lo, tl_hi, warp, lane, accept_union, body);
+                group_sync<WPA>();
+#pragma unroll
+                for (int ch = 0; ch < CELLS / 64; ch++) {
+                    group_reduce64<WPA>(acc + 64 * ch, s, warp, lane);
+                    if (tid == 0) {
+                        int ds = a * a + b * b, base = P.ind4[ds];
+                        for (int f = 0; f < P.ng4; f++) {
+                            int cell = P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam;
+                            if (cell / 64 == ch) s.G[base + f] += s.red[cell % 64];
+                        }
+                    }
+                    group_sync<WPA>();
                 }
-                __syncthreads();
             }
+        if (A.counters) {
+            for (int o = 16; o > 0; o >>= 1) nacc += __shfl_xor_sync(FULL, nacc, o);
+            if (lane == 0) atomicAdd(&A.counters[1], nacc);
         }
+    }
 
     if (A.mode == MB_MODE_DESCRIPTORS) {
         for (int t = tid; t < D; t += NT) A.G[(size_t)i * D + t] = s.G[t];
@@ -607,7 +667,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
             acc = warp_sum(acc);
             if (lane == 0) H1[m] = tanh(b0[m] + acc);
         }
-        __syncthreads();
+        group_sync<WPA>();
         if (warp == 0) {
             double v = 0.0;
             if (lane < h2) {
@@ -628,7 +688,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
                 Dl1[lane] = g * (1.0 - H1[lane] * H1[lane]);
             }
         }
-        __syncthreads();
+        group_sync<WPA>();
         if (A.mode == MB_MODE_ENERGY) return;
         /* s.G <- dE_i/dG_i */
         for (int l = tid; l < D; l += NT) {
@@ -639,7 +699,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
     } else {
         for (int l = tid; l < D; l += NT) s.G[l] = A.G[(size_t)i * D + l];
     }
-    __syncthreads();
+    group_sync<WPA>();
 
     /* ---- reverse pair terms with the species-0 parameters ---- */
     double fi[3] = {0.0, 0.0, 0.0}, vr[6] = {0, 0, 0, 0, 0, 0};
@@ -681,78 +741,79 @@ __global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
             }
         }
     }
-    __syncthreads();
+    group_sync<WPA>();
 
-    /* ---- reverse triplet terms ---- */
-    for (int a = 0; a < ns; a++)
-        for (int b = a; b < ns; b++) {
-            const int ds = a * a + b * b, base = P.ind4[ds];
-            for (int t = tid; t < NE * NZL; t += NT) s.grid[t] = 0.0;
-            __syncthreads();
-            if (tid == 0)
-                for (int f = 0; f < P.ng4; f++)
-                    s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam] += s.G[base + f];
-            __syncthreads();
-            auto accept = [&](int jj, int kk) -> bool {
-                double4 d1 = s.d[jj], d2 = s.d[kk];
-                double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
-                double r3 = sqrt(dx * dx + dy * dy + dz * dz);
-                return d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3 < P.d_rc4;
-            };
-            auto body = [&](int jj, int kk, bool act) {
-                if (!act) return;
-                double4 d1 = s.d[jj], d2 = s.d[kk];
-                double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
-                double r3s = wx * wx + wy * wy + wz * wz, r3 = sqrt(r3s);
-                double r1 = d1.w, r2 = d2.w, ir1 = 1.0 / r1, ir2 = 1.0 / r2, ir3 = 1.0 / r3;
-                double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
-                double f3, df3;
-                fcut_d(P.d_rc4, r3, f3, df3);
-                double f1 = s.fa[jj], df1 = s.fb[jj], f2 = s.fa[kk], df2 = s.fb[kk];
-                double lz[NZL], lzp[NZL];
+    /* ---- reverse triplet terms (list of the forward pass reused) ---- */
+    {
+        const int reuse = (A.mode != MB_MODE_VJP) && tl_whole;
+        int blkid = 0;
+        tl_pos = tl_lo;
+        for (int a = 0; a < ns; a++)
+            for (int b = a; b < ns; b++, blkid++) {
+                const int ds = a * a + b * b, base = P.ind4[ds];
+                for (int t = tid; t < NE * NZL; t += NT) s.grid[t] = 0.0;
+                group_sync<WPA>();
+                if (tid == 0)
+                    for (int f = 0; f < P.ng4; f++)
+                        s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam] += s.G[base + f];
+                group_sync<WPA>();
+                auto body = [&](int jj, int kk) {
+                    double4 d1 = s.d[jj], d2 = s.d[kk];
+                    double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
+                    double r3s = wx * wx + wy * wy + wz * wz;
+                    if (!(d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq)) return;
+                    double r3 = sqrt(r3s);
+                    double r1 = d1.w, r2 = d2.w, ir1 = s.ir[jj], ir2 = s.ir[kk], ir3 = 1.0 / r3;
+                    double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
+                    double f3, df3;
+                    fcut_d(P.d_rc4, r3, f3, df3);
+                    double f1 = s.fa[jj], df1 = s.fb[jj], f2 = s.fa[kk], df2 = s.fb[kk];
+                    double lz[NZL], lzp[NZL];
 #pragma unroll
-                for (int k = 0; k < NZL; k++) { lz[k] = 0.0; lzp[k] = 0.0; }
-                angular<NZ, NLAM>(P, c, lz, lzp);
-                double Q = 0.0, Qe = 0.0, Qc = 0.0;
+                    for (int k = 0; k < NZL; k++) { lz[k] = 0.0; lzp[k] = 0.0; }
+                    angular<NZ, NLAM>(P, c, lz, lzp);
+                    double Q = 0.0, Qe = 0.0, Qc = 0.0;
 #pragma unroll
-                for (int e = 0; e < NE; e++) {
-                    if (e >= ne) break;
-                    double ex = s.P[jj * NE + e] * s.P[kk * NE + e] * exp(-P.d_eta4[e] * r3s);
-                    double u = 0.0, v = 0.0;
+                    for (int e = 0; e < NE; e++) {
+                        if (e >= ne) break;
+                        double ex = s.P[jj * NE + e] * s.P[kk * NE + e] * exp(-P.d_eta4[e] * r3s);
+                        double u = 0.0, v = 0.0;
 #pragma unroll
-                    for (int zl = 0; zl < NZL; zl++) {
-                        double cg = s.grid[e * NZL + zl];
-                        u += cg * lz[zl];
-                        v += cg * lzp[zl];
+                        for (int zl = 0; zl < NZL; zl++) {
+                            double cg = s.grid[e * NZL + zl];
+                            u += cg * lz[zl];
+                            v += cg * lzp[zl];
+                        }
+                        Q += ex * u;
+                        Qe += P.d_eta4[e] * ex * u;
+                        Qc += ex * v;
                     }
-                    Q += ex * u;
-                    Qe += P.d_eta4[e] * ex * u;
-                    Qc += ex * v;
-                }
-                double Af = 2.0 * f1 * f2 * f3;
-                double T1 = 2.0 * df1 * f2 * f3 * Q - 2.0 * r1 * Af * Qe;
-                double T2 = 2.0 * f1 * df2 * f3 * Q - 2.0 * r2 * Af * Qe;
-                double T3 = 2.0 * f1 * f2 * df3 * Q - 2.0 * r3 * Af * Qe;
-                double Tc = Af * Qc;
-                double a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
-                double a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
-                double g1x = a11 * d1.x + a12 * d2.x - a3 * wx, g1y = a11 * d1.y + a12 * d2.y - a3 * wy,
-                       g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
-                double g2x = a22 * d2.x + a12 * d1.x + a3 * wx, g2y = a22 * d2.y + a12 * d1.y + a3 * wy,
-                       g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
-                fi[0] += g1x + g2x; fi[1] += g1y + g2y; fi[2] += g1z + g2z;
-                atomicAdd(&s.Fnb[3 * jj], -g1x); atomicAdd(&s.Fnb[3 * jj + 1], -g1y); atomicAdd(&s.Fnb[3 * jj + 2], -g1z);
-                atomicAdd(&s.Fnb[3 * kk], -g2x); atomicAdd(&s.Fnb[3 * kk + 1], -g2y); atomicAdd(&s.Fnb[3 * kk + 2], -g2z);
-                vr[0] -= g1x * d1.x + g2x * d2.x;
-                vr[1] -= g1y * d1.y + g2y * d2.y;
-                vr[2] -= g1z * d1.z + g2z * d2.z;
-                vr[3] -= g1x * d1.y + g2x * d2.y;
-                vr[4] -= g1y * d1.z + g2y * d2.z;
-                vr[5] -= g1z * d1.x + g2z * d2.x;
-            };
-            for_triplets<WARPS>(s, a, b, warp, lane, accept, body);
-            __syncthreads();
-        }
+                    double Af = 2.0 * f1 * f2 * f3;
+                    double T1 = 2.0 * df1 * f2 * f3 * Q - 2.0 * r1 * Af * Qe;
+                    double T2 = 2.0 * f1 * df2 * f3 * Q - 2.0 * r2 * Af * Qe;
+                    double T3 = 2.0 * f1 * f2 * df3 * Q - 2.0 * r3 * Af * Qe;
+                    double Tc = Af * Qc;
+                    double a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
+                    double a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
+                    double g1x = a11 * d1.x + a12 * d2.x - a3 * wx, g1y = a11 * d1.y + a12 * d2.y - a3 * wy,
+                           g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
+                    double g2x = a22 * d2.x + a12 * d1.x + a3 * wx, g2y = a22 * d2.y + a12 * d1.y + a3 * wy,
+                           g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                    fi[0] += g1x + g2x; fi[1] += g1y + g2y; fi[2] += g1z + g2z;
+                    atomicAdd(&s.Fnb[3 * jj], -g1x); atomicAdd(&s.Fnb[3 * jj + 1], -g1y); atomicAdd(&s.Fnb[3 * jj + 2], -g1z);
+                    atomicAdd(&s.Fnb[3 * kk], -g2x); atomicAdd(&s.Fnb[3 * kk + 1], -g2y); atomicAdd(&s.Fnb[3 * kk + 2], -g2z);
+                    vr[0] -= g1x * d1.x + g2x * d2.x;
+                    vr[1] -= g1y * d1.y + g2y * d2.y;
+                    vr[2] -= g1z * d1.z + g2z * d2.z;
+                    vr[3] -= g1x * d1.y + g2x * d2.y;
+                    vr[4] -= g1y * d1.z + g2y * d2.z;
+                    vr[5] -= g1z * d1.x + g2z * d2.x;
+                };
+                int *blk = s.blk + (blkid * WPA + warp) * 2;
+                for_block<WPA>(s, a, b, blk, reuse, tl_pos, tl_lo, tl_hi, warp, lane, accept_union, body);
+                group_sync<WPA>();
+            }
+    }
 
     /* ---- write forces and the virial of atom i ---- */
     {
@@ -762,7 +823,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_efs(EfsArgs A) {
         v[0] = fi[0]; v[1] = fi[1]; v[2] = fi[2];
 #pragma unroll
         for (int k = 0; k < 6; k++) v[3 + k] = vr[k];
-        cta_reduce64<WARPS>(v, s, warp, lane);
+        group_reduce64<WPA>(v, s, warp, lane);
         if (tid == 0) {
             atomicAdd(&A.F[3 * i], s.red[0]);
             atomicAdd(&A.F[3 * i + 1], s.red[1]);
@@ -868,16 +929,37 @@ __global__ void k_set_out(double *out, int idx, double v) { out[idx] = v; }
 /* launchers                                                           */
 /* ------------------------------------------------------------------ */
 
-#define MB_EFS_WARPS 4
+/* Shapes of the fused kernel: warps per atom x atoms per block.  One warp
+ * per atom keeps many atoms resident per SM (large structures); several
+ * warps per atom shorten the latency of small structures. */
+struct EfsShape {
+    int wpa, apb;
+};
+static const EfsShape kShapes[] = {{1, 4}, {4, 1}, {8, 1}};
+#define MB_NSHAPES 3
 
 /* specialised kernel for the reference bases: 7 G4 exponents, 4 zeta, 2 lambda */
 static bool efs_fast(const mb_model *m) { return m->P.ne <= 7 && m->P.nz <= 4 && m->P.nlam <= 2; }
 
-extern "C" size_t mbk_efs_smem(const mb_model *m, int capNB, int warps) {
+/* triplet-list entries per atom group: all candidate pairs when they fit,
+ * otherwise at least one row (the capacity) per warp plus slack */
+static int tl_entries(int capNB, int wpa) {
+    int all = capNB * (capNB - 1) / 2 + 32 * wpa;
+    int lim = wpa == 1 ? 2048 : 8192;
+    int floor_ = wpa * (capNB + 64);
+    int v = all < lim ? all : lim;
+    return v > floor_ ? v : floor_;
+}
+
+static size_t group_bytes(const mb_model *m, int capNB, int wpa) {
     bool fast = efs_fast(m);
     int ne = fast ? 7 : MB_MAXE;
     int cells = fast ? 7 * 8 : MB_MAXE * 8 * 4;
-    return efs_smem_bytes(capNB, m->P.D, ne, m->P.ng2, cells, warps);
+    return (efs_smem_bytes(capNB, m->P.D, ne, m->P.ng2, cells, wpa, tl_entries(capNB, wpa)) + 15) & ~(size_t)15;
+}
+
+extern "C" size_t mbk_efs_smem(const mb_model *m, int capNB, int shape) {
+    return group_bytes(m, capNB, kShapes[shape].wpa) * kShapes[shape].apb;
 }
 
 extern "C" int mbk_wrap(mb_dev *d, int N, const mb_cell *c, void *stream, long *launches) {
@@ -912,19 +994,80 @@ extern "C" int mbk_nlist(mb_dev *d, int N, int NM, const mb_cell *c, double rc, 
     return (int)cudaGetLastError();
 }
 
-template <int NE, int NZ, int NLAM>
-static int launch_efs(const EfsArgs &a, size_t smem, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
-    auto kern = k_efs<NE, NZ, NLAM, MB_EFS_WARPS>;
+template <int NE, int NZ, int NLAM, int WPA, int APB>
+static int launch_shape(const EfsArgs &a, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
+    auto kern = k_efs<NE, NZ, NLAM, WPA, APB>;
+    size_t smem = a.smem_group * APB;
     static size_t configured = 0;
+    if (smem > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
     if (smem > 48 * 1024 && smem > configured) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
         configured = smem;
     }
     if (e0) cudaEventRecord(e0, st);
-    kern<<<a.N, MB_EFS_WARPS * 32, smem, st>>>(a);
+    kern<<<(a.N + APB - 1) / APB, WPA * 32 * APB, smem, st>>>(a);
     if (e1) cudaEventRecord(e1, st);
     return (int)cudaGetLastError();
+}
+
+static int launch_any(const mb_model *m, int shape, EfsArgs a, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
+    a.smem_group = group_bytes(m, a.cap, kShapes[shape].wpa);
+    a.tl_cap = tl_entries(a.cap, kShapes[shape].wpa);
+    if (efs_fast(m)) {
+        switch (shape) {
+            case 0: return launch_shape<7, 4, 2, 1, 4>(a, st, e0, e1);
+            case 1: return launch_shape<7, 4, 2, 4, 1>(a, st, e0, e1);
+            default: return launch_shape<7, 4, 2, 8, 1>(a, st, e0, e1);
+        }
+    }
+    if (m->P.nz > 8 || m->P.nlam > 4) return (int)cudaErrorInvalidValue;
+    switch (shape) {
+        case 0: return launch_shape<MB_MAXE, 8, 4, 1, 4>(a, st, e0, e1);
+        case 1: return launch_shape<MB_MAXE, 8, 4, 4, 1>(a, st, e0, e1);
+        default: return launch_shape<MB_MAXE, 8, 4, 8, 1>(a, st, e0, e1);
+    }
+}
+
+/* Autotuner: on the first pass of a (mode, size bucket, capacity) the three
+ * shapes are each timed once (after an untimed launch) and the fastest is
+ * kept for later passes of that key. */
+static int tune_shape(mb_dev *d, const mb_model *m, int N, int mode, const EfsArgs &a, cudaStream_t st) {
+    int bucket = 0, k;
+    while ((1 << bucket) < N) bucket++;
+    int key = (mode << 28) | (bucket << 20) | (d->capNB & 0xfffff);
+    for (k = 0; k < d->tune_n; k++)
+        if (d->tune_key[k] == key) return d->tune_val[k];
+    if (d->tune_fixed >= 0) return d->tune_fixed;
+    EfsArgs t = a;
+    t.counters = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = 0;
+    float best_ms = 1e30f;
+    for (int sh = 0; sh < MB_NSHAPES; sh++) {
+        if (group_bytes(m, a.cap, kShapes[sh].wpa) * kShapes[sh].apb > 227 * 1024) continue;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+            if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
+            if (launch_any(m, sh, t, st, rep ? e0 : nullptr, rep ? e1 : nullptr)) break;
+        }
+        if (cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = sh;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGetLastError();
+    if (d->tune_n < MB_TUNE_SLOTS) {
+        d->tune_key[d->tune_n] = key;
+        d->tune_val[d->tune_n] = best;
+        d->tune_n++;
+    }
+    return best;
 }
 
 extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode, double urep, int need_nb_max,
@@ -949,23 +1092,18 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
     a.F = d->F;
     a.vir = d->vir;
     a.counters = d->counters;
+    a.smem_group = 0;
+    cudaMemsetAsync(d->EU, 0, sizeof(double) * N, st);
+    int shape = tune_shape(d, m, N, mode, a, st);
+    d->last_shape = shape;
     cudaEvent_t e0 = 0, e1 = 0;
     if (d->ev_on && d->ev_n < d->ev_cap) {
         e0 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n];
         e1 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n + 1];
         d->ev_n++;
     }
-    cudaMemsetAsync(d->EU, 0, sizeof(double) * N, st);
     if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
-    size_t smem = mbk_efs_smem(m, d->capNB, MB_EFS_WARPS);
-    int rc;
-    if (smem > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
-    if (efs_fast(m))
-        rc = launch_efs<7, 4, 2>(a, smem, st, e0, e1);
-    else if (m->P.nz <= 8 && m->P.nlam <= 4)
-        rc = launch_efs<MB_MAXE, 8, 4>(a, smem, st, e0, e1);
-    else
-        rc = (int)cudaErrorInvalidValue;
+    int rc = launch_any(m, shape, a, st, e0, e1);
     (*launches)++;
     return rc;
 }

@@ -79,6 +79,11 @@ int mb_open(const char *model_path, int device, mb_potential **out) {
         return fail(MB_ERR_MODEL, "%s", err);
     }
     p->device = device;
+    p->d.tune_fixed = -1;
+    {
+        const char *fx = getenv("MAISE_B200_SHAPE");
+        if (fx) p->d.tune_fixed = atoi(fx);
+    }
     CK(cudaSetDevice(device), "cudaSetDevice");
     CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     CK(cudaMalloc((void **)&p->d.params, sizeof(mb_params)), "cudaMalloc params");
@@ -672,6 +677,8 @@ int mb_md_nvt(mb_potential *p, int N, int NM, int ND, const int *atmn, const dou
         return fail(MB_ERR_ARG, "bad arguments");
     CK(cudaSetDevice(p->device), "cudaSetDevice");
     setup_cell(p, lat9, ND, N, &c);
+    if ((r = ensure(p, N, p->d.capNB ? p->d.capNB : (NM < 64 ? NM : 64), c.M[0] ? c.M[0] * c.M[1] * c.M[2] : 1)))
+        return r;
     if ((r = upload(p, N, 1, atmn, lat9, x))) return r;
     CK(cudaMemcpyAsync(p->d.V, v, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, p->stream), "H2D velocities");
     if (p->d.capTrace < nsteps) {

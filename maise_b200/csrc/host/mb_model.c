@@ -259,6 +259,7 @@ static int parse_basis(const mb_lines *L, mb_model *m, char *err, size_t el) {
                 p = s * s + t * t;
                 P->f_rc2[p] = W->gp[0][gf[0][1]];
                 P->f_rc4[p] = P->ng4 ? W->gp[0][gf[g4first][1]] : 0.0;
+                P->f_rc4sq[p] = P->f_rc4[p] * P->f_rc4[p];
                 for (f = 0; f < P->ng2; f++) {
                     P->f_eta2[p][f] = W->gp[2][gf[f][3]];
                     P->f_rs[p][f] = W->gp[1][gf[f][2]];
@@ -267,6 +268,7 @@ static int parse_basis(const mb_lines *L, mb_model *m, char *err, size_t el) {
             }
         P->d_rc2 = blk[0].gp[0][gf[0][1]];
         P->d_rc4 = P->ng4 ? blk[0].gp[0][gf[g4first][1]] : 0.0;
+        P->d_rc4sq = P->d_rc4 * P->d_rc4;
         for (f = 0; f < P->ng2; f++) {
             P->d_eta2[f] = blk[0].gp[2][gf[f][3]];
             P->d_rs[f] = blk[0].gp[1][gf[f][2]];

@@ -30,11 +30,11 @@ typedef struct {
     int nspc, D, ng2, ng4, ne, nz, nlam, nzl, h1, h2;
     int ind2[4], ind4[20];
     /* forward parameters per pair index p = s0*s0+s1*s1 */
-    double f_rc2[MB_NPAIR], f_rc4[MB_NPAIR];
+    double f_rc2[MB_NPAIR], f_rc4[MB_NPAIR], f_rc4sq[MB_NPAIR];
     double f_eta2[MB_NPAIR][MB_MAXG2], f_rs[MB_NPAIR][MB_MAXG2];
     double f_eta4[MB_NPAIR][MB_MAXE];
     /* derivative parameters (species-0 block) */
-    double d_rc2, d_rc4;
+    double d_rc2, d_rc4, d_rc4sq;
     double d_eta2[MB_MAXG2], d_rs[MB_MAXG2], d_eta4[MB_MAXE];
     /* angular parameters (species-0 block) */
     double zeta[MB_MAXZ], lam[MB_MAXL], powz[MB_MAXZ];
@@ -125,6 +125,10 @@ typedef struct {
     void *st_pool;    /* cudaEvent_t[2*st_cap] */
     void *flush;
     size_t flush_bytes;
+    /* kernel-shape autotuner cache (see mb_kernels.cu) */
+#define MB_TUNE_SLOTS 32
+    int tune_n, tune_fixed, last_shape;
+    int tune_key[MB_TUNE_SLOTS], tune_val[MB_TUNE_SLOTS];
 } mb_dev;
 
 /* Launchers (mb_kernels.cu).  All enqueue on `stream`; return 0 or a CUDA
@@ -137,7 +141,7 @@ int mbk_finalize(mb_dev *d, int N, int mode, double pV, void *stream, long *laun
 int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, int step, void *stream,
                    long *launches);
 int mbk_set_xi(mb_dev *d, double xi, void *stream);
-size_t mbk_efs_smem(const mb_model *m, int capNB, int warps);
+size_t mbk_efs_smem(const mb_model *m, int capNB, int shape);
 
 #ifdef __cplusplus
 }

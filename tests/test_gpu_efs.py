@@ -119,7 +119,7 @@ for k in range(2):
                        LAT.ctypes.data_as(D), X.ctypes.data_as(D), F.ctypes.data_as(D), S.ctypes.data_as(D))
     assert ctypes.c_int.from_buffer(L, 152).value == 1
     assert ctypes.c_double.from_buffer(C, 1768).value == H
-print(repr(H), *map(repr, F), *map(repr, S))
+print(repr(float(H)), *[repr(float(v)) for v in F], *[repr(float(v)) for v in S])
 """
     out = subprocess.run([sys.executable, "-c", script], cwd=d, capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr

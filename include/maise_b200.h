@@ -97,6 +97,28 @@ int mb_descriptor_vjp(mb_potential *pot, int N, int NM, int ND, int XT, const in
 int mb_relax(mb_potential *pot, int N, int NM, int ND, const int *atmn, double *lat9, double *x, double p_gpa,
              double urep, int rlxt, int mitr, double etol, double *H, long *counts);
 
+/* mb_relax with the force criterion of mb_relax_batch instead of the
+ * enthalpy change: stops when max |F| < fmax and max |U - pV| / N < fmax,
+ * or after mitr iterations.  Returns MB_OK; *converged tells which. */
+int mb_relax_fmax(mb_potential *pot, int N, int NM, int ND, const int *atmn, double *lat9, double *x, double p_gpa,
+                  double urep, int rlxt, int mitr, double fmax, double *H, long *counts, int *converged);
+
+/* Relaxation of a population of independent structures in one persistent
+ * launch: the batched counterpart of the evolutionary search's serial
+ * relaxation loop (RELX_INT, src/emod.c:521-548, each member through
+ * CELL_RELX).  Structure s has nat[s] <= 64 atoms; its atoms are rows
+ * off[s] .. off[s]+nat[s]-1 of atmn and x (off = exclusive prefix sum of
+ * nat); lat[9*s] is its lattice.  Every structure is relaxed on the device
+ * by BFGS with Fletcher's line search over the DOF vector of rlxt (2 or 3),
+ * FP64 state, with descriptors and MLP in FP32 and FP64 energy and virial
+ * reductions.  A structure stops when max |F| < fmax (eV/A) and
+ * max |U_ab - pV delta_ab| / N < fmax (eV), or after mitr iterations.
+ * x (Cartesian) and lat are updated in place; H[s] gets the enthalpy,
+ * iters[s] the iterations and status[s] 0 (converged), 1 (iteration limit),
+ * 2 (too many neighbours), 3 (no descent possible). */
+int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, double *lat, double *x, double p_gpa,
+                   double urep, int rlxt, int mitr, double fmax, double *H, int *iters, int *status);
+
 /* NVT molecular dynamics with the reference's thermostat (the RUNT == 2
  * branch of Dynamics, src/cmod.c:403-407, 440-453), entirely on the GPU:
  * per step  E+F+S -> K -> xi += dt/tau^2 (2K/(3 N T) - 1)
@@ -139,6 +161,10 @@ int mb_md_profile(mb_potential *pot, int enable, int capacity, size_t flush_byte
 
 /* Summed step time (ms) and number of timed steps since mb_md_profile(pot, 1, ...). */
 int mb_md_profile_read(mb_potential *pot, double *total_ms, int *steps);
+
+/* Energy+gradient evaluations and kernel time (ms) of the last
+ * mb_relax_batch call on this handle. */
+int mb_batch_stats(const mb_potential *pot, long long *evals, double *ms);
 
 /* Sustained FP64 FMA throughput of `device` in TFLOP/s, measured with an
  * FMA-chain kernel over every SM (a roofline denominator for FP64 work). */

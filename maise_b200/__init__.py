@@ -58,6 +58,9 @@ def load_library():
     lib.mb_relax.argtypes = [vp, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _D, _L]
     lib.mb_md_nvt.argtypes = [vp, c_i, c_i, c_i, _I, _D, _D, _D, c_d, c_d, c_d, c_i, c_d, _D, _D, _D]
     lib.mb_maxwell.argtypes = [c_i, _D, c_d, ctypes.c_long, _D]
+    lib.mb_relax_fmax.argtypes = [vp, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _D, _L, _I]
+    lib.mb_relax_batch.argtypes = [vp, c_i, _I, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _D, _I, _I]
+    lib.mb_batch_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), _D]
     lib.mb_atomic_mass.restype = c_d
     lib.mb_atomic_mass.argtypes = [c_i]
     lib.mb_stream.restype = vp
@@ -247,6 +250,41 @@ class Potential:
                                       rlxt, mitr, etol, ctypes.byref(H), counts.ctypes.data_as(_L)))
         return dict(H=H.value, X=X.reshape(N, 3), LAT=LAT.reshape(3, 3), n_energy=int(counts[0]),
                     n_force=int(counts[1]), iters=int(counts[2]))
+
+    def relax_fmax(self, X, LAT, atmn, ND=3, NM=512, p_gpa=0.0, urep=0.0, rlxt=3, mitr=500, fmax=0.01):
+        """dict(H, X, LAT, n_energy, n_force, iters, converged) -- force-criterion relax, FP64, host BFGS."""
+        atmn = _i32(atmn)
+        N = len(atmn)
+        X = _f64(X, 3 * N).copy()
+        LAT = _f64(LAT, 9).copy()
+        H = ctypes.c_double()
+        counts = np.zeros(3, np.int64)
+        conv = ctypes.c_int()
+        self._check(self.lib.mb_relax_fmax(self.h, N, NM, ND, atmn.ctypes.data_as(_I), _dp(LAT), _dp(X), p_gpa, urep,
+                                           rlxt, mitr, fmax, ctypes.byref(H), counts.ctypes.data_as(_L),
+                                           ctypes.byref(conv)))
+        return dict(H=H.value, X=X.reshape(N, 3), LAT=LAT.reshape(3, 3), n_energy=int(counts[0]),
+                    n_force=int(counts[1]), iters=int(counts[2]), converged=bool(conv.value))
+
+    def relax_batch(self, structures, p_gpa=0.0, urep=0.0, rlxt=3, mitr=500, fmax=0.01):
+        """Relax a list of dict(X, LAT, atmn) in one persistent launch.
+        Returns dict(H[S], X list, LAT[S,3,3], iters[S], status[S], evals, ms)."""
+        nat = np.array([len(s["atmn"]) for s in structures], np.int32)
+        atmn = np.ascontiguousarray(np.concatenate([np.asarray(s["atmn"], np.int32) for s in structures]))
+        X = np.ascontiguousarray(np.concatenate([np.asarray(s["X"], float).reshape(-1, 3) for s in structures]))
+        LAT = np.ascontiguousarray(np.stack([np.asarray(s["LAT"], float).reshape(3, 3) for s in structures]))
+        S = len(structures)
+        H = np.zeros(S)
+        iters = np.zeros(S, np.int32)
+        status = np.zeros(S, np.int32)
+        self._check(self.lib.mb_relax_batch(self.h, S, nat.ctypes.data_as(_I), atmn.ctypes.data_as(_I), _dp(LAT),
+                                            _dp(X), p_gpa, urep, rlxt, mitr, fmax, _dp(H),
+                                            iters.ctypes.data_as(_I), status.ctypes.data_as(_I)))
+        ev, ms = ctypes.c_longlong(), ctypes.c_double()
+        self._check(self.lib.mb_batch_stats(self.h, ctypes.byref(ev), ctypes.byref(ms)))
+        offs = np.concatenate([[0], np.cumsum(nat)])
+        return dict(H=H, X=[X[offs[k]:offs[k + 1]] for k in range(S)], LAT=LAT, iters=iters, status=status,
+                    evals=int(ev.value), ms=float(ms.value))
 
     def maxwell(self, atmn, T, seed=1):
         """Initial velocities of the reference's Maxwell() for model species atmn."""

@@ -1,0 +1,1008 @@
+/*
+ * mb_batch.cu -- relaxation of a population of small structures in one
+ * persistent launch (the batched counterpart of RELX_INT's serial loop,
+ * src/emod.c:521-548).
+ *
+ * Each CTA takes structures from an atomic work counter and relaxes each
+ * one completely on the device:
+ *   - BFGS over the DOF vector of CELL_MIN (fractional coordinates, then
+ *     the nine lattice components, src/cmin.c:22-88), FP64 state: the
+ *     inverse Hessian in per-CTA global scratch, the vectors in shared
+ *     memory; Fletcher's line search (Algorithms 2.6.2/2.6.4) driven by
+ *     thread 0 with the CTA evaluating every trial point;
+ *   - each evaluation: wrap, brute-force periodic neighbour list (FP64
+ *     displacements), and per atom (one warp each) the G2/G4 descriptors,
+ *     MLP and reverse pass in FP32, with forces gathered in shared memory and
+ *     energy and virial reduced in FP64; the repulsion term in FP64;
+ *   - the gradient of cdfunc_gsl (src/cmin.c:107-166) in FP64.
+ * A structure stops when max |F| < fmax and max |U - pV| / N < fmax.
+ */
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "../../../include/maise_b200.h"
+#include "../mb_internal.h"
+
+#define FULLM 0xffffffffu
+
+namespace {
+
+constexpr int BMAXN = 64;
+constexpr int BMAXNB = 96;
+constexpr int BMAXDOF = 3 * BMAXN + 9;
+constexpr int BMAXD = 288;
+constexpr int BTL = 1024;
+constexpr int BWARPS = 4;
+constexpr int BNE = 7, BNZ = 4, BNLAM = 2, BNZL = 8, BCELLS = 64;
+
+/* FP32 copy of the descriptor parameters (fast basis layout only) */
+struct BParams {
+    int nspc, D, ng2, ng4, ne, nz, nlam, h1, h2;
+    int ind2[4], ind4[20];
+    float f_rc2[MB_NPAIR], f_rc4[MB_NPAIR], f_rc4sq[MB_NPAIR];
+    float f_eta2[MB_NPAIR][MB_MAXG2], f_rs[MB_NPAIR][MB_MAXG2], f_eta4[MB_NPAIR][MB_MAXE];
+    float d_rc2, d_rc4, d_rc4sq;
+    float d_eta2[MB_MAXG2], d_rs[MB_MAXG2], d_eta4[MB_MAXE];
+    float lam[MB_MAXL], powz[MB_MAXZ], zeta[MB_MAXZ];
+    int zbits[MB_MAXZ], zm1bits[MB_MAXZ];
+    int g4_cell[MB_MAXG4];
+    double rm[MB_MAXSPC];
+    double rc;
+    int w_off[MB_MAXSPC];
+};
+
+struct BArgs {
+    int S, rlxt, mitr;
+    double p_ev, urep, fmax, sigma;
+    const int *nat, *off, *spc;
+    double *lat, *x, *H;
+    int *iters, *status;
+    const BParams *P;
+    const float *W;
+    int *queue;
+    double *hmat;  /* per CTA: BMAXDOF^2 */
+    float4 *nbd;   /* per CTA: BMAXN * BMAXNB */
+    int *nbj;      /* per CTA: BMAXN * BMAXNB */
+    long long *evals;
+};
+
+struct WarpWS {
+    float4 d[BMAXNB];
+    float ir[BMAXNB], fa[BMAXNB], fb[BMAXNB];
+    float P[BMAXNB * BNE];
+    float Fnb[BMAXNB * 3];
+    float grid[BCELLS];
+    float G[BMAXD];
+    float h[4 * MB_MAXH];
+    double red[64];
+    int j[BMAXNB], sp[BMAXNB], raw[BMAXNB];
+    unsigned tl[BTL];
+    int blk[6][2];
+    int seg[8];
+};
+
+struct BShared {
+    double L[9], R[9];
+    double xc[BMAXN * 3];
+    double ea[BMAXN], eu[BMAXN];
+    double x[BMAXDOF], g[BMAXDOF], p[BMAXDOF], xt[BMAXDOF], gt[BMAXDOF], xa[BMAXDOF], ga[BMAXDOF], hy[BMAXDOF];
+    double vir[BWARPS][6];
+    double uvir[6];
+    double red[BWARPS * 32];
+    double scal[24];
+    float F[BMAXN * 3];
+    int spc[BMAXN];
+    int nn[BMAXN];
+    int s, N, ndof, flag, cmd, first;
+    WarpWS ws[BWARPS];
+};
+
+/* ---------------- small helpers ---------------- */
+
+__device__ __forceinline__ float fcutf(float rc, float r) { return r > rc ? 0.0f : 0.5f * (cospif(r / rc) + 1.0f); }
+
+__device__ __forceinline__ void fcutf_d(float rc, float r, float &f, float &df) {
+    if (r > rc) {
+        f = 0.0f;
+        df = 0.0f;
+        return;
+    }
+    float s, c;
+    sincospif(r / rc, &s, &c);
+    f = 0.5f * (c + 1.0f);
+    df = -0.5f * CUDART_PI_F / rc * s;
+}
+
+__device__ __forceinline__ void angularf(const BParams &P, float c, float *lz, float *lzp) {
+#pragma unroll
+    for (int l = 0; l < BNLAM; l++) {
+        float lam = P.lam[l], base = 1.0f + lam * c;
+        float sq[7];
+        sq[0] = base;
+#pragma unroll
+        for (int k = 1; k < 7; k++) sq[k] = sq[k - 1] * sq[k - 1];
+#pragma unroll
+        for (int z = 0; z < BNZ; z++) {
+            int zb = P.zbits[z], mb = P.zm1bits[z];
+            float pw = 1.0f, pm = 1.0f;
+#pragma unroll
+            for (int k = 0; k < 7; k++) {
+                if (zb & (1 << k)) pw *= sq[k];
+                if (mb & (1 << k)) pm *= sq[k];
+            }
+            lz[z * BNLAM + l] = P.powz[z] * pw;
+            if (lzp) lzp[z * BNLAM + l] = P.powz[z] * P.zeta[z] * lam * pm;
+        }
+    }
+}
+
+__device__ __forceinline__ double bsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULLM, v, o);
+    return v;
+}
+__device__ __forceinline__ float bsumf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULLM, v, o);
+    return v;
+}
+
+/* CTA-wide sum of one double per thread (all threads get the result) */
+__device__ double cta_sum(BShared &sh, double v) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v = bsum(v);
+    __syncthreads();
+    if (lane == 0) sh.red[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int k = 0; k < BWARPS; k++) t += sh.red[k];
+    __syncthreads();
+    return t;
+}
+
+__device__ double cta_max(BShared &sh, double v) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULLM, v, o));
+    __syncthreads();
+    if (lane == 0) sh.red[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int k = 0; k < BWARPS; k++) t = fmax(t, sh.red[k]);
+    __syncthreads();
+    return t;
+}
+
+__device__ void reciprocal9(const double *L, double *R) {
+    R[6] = L[1] * L[5] - L[2] * L[4];
+    R[7] = L[2] * L[3] - L[0] * L[5];
+    R[8] = L[0] * L[4] - L[1] * L[3];
+    R[0] = L[4] * L[8] - L[5] * L[7];
+    R[1] = L[5] * L[6] - L[3] * L[8];
+    R[2] = L[3] * L[7] - L[4] * L[6];
+    R[3] = L[7] * L[2] - L[8] * L[1];
+    R[4] = L[8] * L[0] - L[6] * L[2];
+    R[5] = L[6] * L[1] - L[7] * L[0];
+    double t = 1.0 / (L[0] * L[4] * L[8] + L[1] * L[5] * L[6] + L[2] * L[3] * L[7] - L[0] * L[5] * L[7] -
+                      L[1] * L[3] * L[8] - L[2] * L[4] * L[6]);
+    for (int k = 0; k < 9; k++) R[k] *= t;
+}
+
+/* triplet list gate: the union of the forward and derivative gates */
+__device__ __forceinline__ bool tgate(const BParams &P, const WarpWS &ws, int s0, int jj, int kk) {
+    float4 d1 = ws.d[jj], d2 = ws.d[kk];
+    int sj = ws.sp[jj], sk = ws.sp[kk];
+    int p01 = s0 * s0 + sj * sj, p02 = s0 * s0 + sk * sk, p12 = sj * sj + sk * sk;
+    float dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+    float r3s = dx * dx + dy * dy + dz * dz;
+    bool fwd = d1.w < P.f_rc2[p01] && d1.w < P.f_rc4[p01] && d2.w < P.f_rc4[p02] && r3s < P.f_rc4sq[p12];
+    bool rev = d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq;
+    return fwd || rev;
+}
+
+/* ---------------- one atom: descriptors, MLP, reverse pass (FP32) ---------------- */
+
+__device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const float4 *nbd, const int *nbj,
+                          double *virw) {
+    const BParams &P = *A.P;
+    const int lane = threadIdx.x & 31;
+    const int n = sh.nn[i], s0 = sh.spc[i], ns = P.nspc, D = P.D, ng2 = P.ng2;
+    /* stage neighbours sorted by relative species */
+    for (int t = lane; t < n; t += 32) ws.raw[t] = sh.spc[nbj[i * BMAXNB + t]];
+    __syncwarp();
+    if (lane == 0) {
+        int cnt[4] = {0, 0, 0, 0};
+        for (int t = 0; t < n; t++) cnt[(ws.raw[t] - s0 + ns) % ns]++;
+        int o = 0;
+        for (int v = 0; v < 4; v++) {
+            ws.seg[v] = cnt[v];
+            ws.seg[4 + v] = o;
+            o += cnt[v];
+        }
+    }
+    for (int t = lane; t < D; t += 32) ws.G[t] = 0.0f;
+    __syncwarp();
+    for (int t = lane; t < n; t += 32) {
+        int ds = (ws.raw[t] - s0 + ns) % ns, rank = 0;
+        for (int u = 0; u < t; u++) rank += ((ws.raw[u] - s0 + ns) % ns) == ds;
+        int dst = ws.seg[4 + ds] + rank;
+        float4 dv = nbd[i * BMAXNB + t];
+        ws.d[dst] = dv;
+        ws.ir[dst] = 1.0f / dv.w;
+        ws.j[dst] = nbj[i * BMAXNB + t];
+        ws.sp[dst] = ws.raw[t];
+    }
+    __syncwarp();
+
+    /* forward pairs: G2 sums per relative species (lane accumulators, warp sums) */
+    float g2acc[3][16];
+#pragma unroll
+    for (int v = 0; v < 3; v++)
+#pragma unroll
+        for (int f = 0; f < 16; f++) g2acc[v][f] = 0.0f;
+    double eu = 0.0;
+    for (int t = lane; t < n; t += 32) {
+        float4 dv = ws.d[t];
+        float r = dv.w;
+        int sj = ws.sp[t], p = s0 * s0 + sj * sj, ds1 = (sj - s0 + ns) % ns;
+        float fa = fcutf(P.f_rc2[p], r);
+        ws.fa[t] = fa;
+        ws.fb[t] = fcutf(P.f_rc4[p], r);
+#pragma unroll
+        for (int e = 0; e < BNE; e++) ws.P[t * BNE + e] = e < P.ne ? expf(-P.f_eta4[p][e] * r * r) : 0.0f;
+        if (r < P.f_rc2[p]) {
+#pragma unroll
+            for (int f = 0; f < 16; f++) {
+                if (f < ng2) {
+                    float x = r - P.f_rs[p][f];
+                    float val = fa * expf(-P.f_eta2[p][f] * (x * x));
+#pragma unroll
+                    for (int v = 0; v < 3; v++)
+                        if (v == ds1) g2acc[v][f] += val;
+                }
+            }
+        }
+        if (A.urep > 0.0) {
+            double R = P.rm[s0] + P.rm[sj], rd = (double)r;
+            if (rd < R) eu += A.urep * 0.5 * (1.0 + cospi(rd / R)) * R / rd;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 3; v++)
+#pragma unroll
+        for (int f = 0; f < 16; f++) {
+            float t = bsumf(g2acc[v][f]);
+            if (lane == 0 && v < ns && f < ng2) ws.G[P.ind2[v] + f] = t;
+        }
+    eu = bsum(eu);
+    if (lane == 0) sh.eu[i] = eu;
+    __syncwarp();
+
+    /* triplets: per species block, list of accepted (j,k), FP32 terms, lane accumulators */
+    int tl_pos = 0, whole = 1, blkid = 0;
+    for (int a = 0; a < ns; a++)
+        for (int b = a; b < ns; b++, blkid++) {
+            float acc[BCELLS];
+#pragma unroll
+            for (int k = 0; k < BCELLS; k++) acc[k] = 0.0f;
+            const int na = ws.seg[a], nb = ws.seg[b], oa = ws.seg[4 + a], ob = ws.seg[4 + b];
+            int row = 0, start = tl_pos;
+            for (;;) {
+                int from = tl_pos;
+                for (; row < na; row++) {
+                    int jj = oa + row, k0 = (a == b) ? row + 1 : 0;
+                    if (tl_pos + (nb - k0) > BTL) break;
+                    for (int kb = k0; kb < nb; kb += 32) {
+                        int kk = ob + kb + lane;
+                        bool ok = false;
+                        if (kb + lane < nb) ok = tgate(P, ws, s0, jj, kk);
+                        unsigned m = __ballot_sync(FULLM, ok);
+                        if (ok) ws.tl[tl_pos + __popc(m & ((1u << lane) - 1u))] = (unsigned)jj | ((unsigned)kk << 16);
+                        tl_pos += __popc(m);
+                    }
+                }
+                __syncwarp();
+                for (int t = from + lane; t < tl_pos; t += 32) {
+                    unsigned pk = ws.tl[t];
+                    int jj = pk & 0xffff, kk = pk >> 16;
+                    float4 d1 = ws.d[jj], d2 = ws.d[kk];
+                    int sj = ws.sp[jj], sk = ws.sp[kk], p12 = sj * sj + sk * sk;
+                    int p01 = s0 * s0 + sj * sj, p02 = s0 * s0 + sk * sk;
+                    float dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+                    float r3s = dx * dx + dy * dy + dz * dz, r3 = sqrtf(r3s);
+                    if (!(d1.w < P.f_rc2[p01] && d1.w < P.f_rc4[p01] && d2.w < P.f_rc4[p02] && r3s < P.f_rc4sq[p12]))
+                        continue;
+                    float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ws.ir[jj] * ws.ir[kk]);
+                    float A3 = 2.0f * ws.fa[jj] * ws.fb[kk] * fcutf(P.f_rc4[p12], r3);
+                    float lz[BNZL];
+                    angularf(P, c, lz, nullptr);
+#pragma unroll
+                    for (int e = 0; e < BNE; e++) {
+                        float ex = A3 * ws.P[jj * BNE + e] * ws.P[kk * BNE + e] * expf(-P.f_eta4[p12][e] * r3s);
+#pragma unroll
+                        for (int zl = 0; zl < BNZL; zl++) acc[e * BNZL + zl] += ex * lz[zl];
+                    }
+                }
+                __syncwarp();
+                if (row >= na) break;
+                whole = 0;
+                start = tl_pos = 0;
+            }
+            ws.blk[blkid][0] = start;
+            ws.blk[blkid][1] = tl_pos;
+            /* lane sums in FP64 across the warp */
+            for (int cell = 0; cell < BCELLS; cell++) {
+                double t = bsum((double)acc[cell]);
+                if (lane == 0) ws.red[cell] = t;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                int base = P.ind4[a * a + b * b];
+                for (int f = 0; f < P.ng4; f++) ws.G[base + f] += (float)ws.red[P.g4_cell[f]];
+            }
+            __syncwarp();
+        }
+
+    /* MLP forward and dE/dG (src/nmlp.c:367-431) */
+    const int h1 = P.h1, h2 = P.h2;
+    const float *net = A.W + P.w_off[s0];
+    const float *off = net, *W0 = off + D, *b0 = W0 + h1 * D, *W1 = b0 + h1, *b1 = W1 + h2 * h1, *W2 = b1 + h2,
+                *b2 = W2 + h2;
+    float *H1 = ws.h, *Dl1 = ws.h + 2 * MB_MAXH;
+    for (int m = 0; m < h1; m++) {
+        float acc = 0.0f;
+        for (int l = lane; l < D; l += 32) acc += (ws.G[l] - off[l]) * W0[m * D + l];
+        acc = bsumf(acc);
+        if (lane == 0) H1[m] = tanhf(b0[m] + acc);
+    }
+    __syncwarp();
+    float v = 0.0f;
+    if (lane < h2) {
+        v = b1[lane];
+        for (int k = 0; k < h1; k++) v += H1[k] * W1[lane * h1 + k];
+        v = tanhf(v);
+    }
+    float e = lane < h2 ? v * W2[lane] : 0.0f;
+    e = bsumf(e);
+    if (lane == 0) sh.ea[i] = (double)b2[0] + (double)e;
+    float dl2 = lane < h2 ? W2[lane] * (1.0f - v * v) : 0.0f;
+    float dl1 = 0.0f;
+    for (int m = 0; m < h2; m++) {
+        float t = __shfl_sync(FULLM, dl2, m);
+        if (lane < h1) dl1 += t * W1[m * h1 + lane];
+    }
+    if (lane < h1) Dl1[lane] = dl1 * (1.0f - H1[lane] * H1[lane]);
+    __syncwarp();
+    for (int l = lane; l < D; l += 32) {
+        float g = 0.0f;
+        for (int k = 0; k < h1; k++) g += Dl1[k] * W0[k * D + l];
+        ws.G[l] = g;
+    }
+    __syncwarp();
+
+    /* reverse pairs (species-0 derivative parameters) */
+    float fi0 = 0.0f, fi1 = 0.0f, fi2 = 0.0f;
+    double vr[6] = {0, 0, 0, 0, 0, 0};
+    for (int t = lane; t < n; t += 32) {
+        float4 d = ws.d[t];
+        float r = d.w, ir = ws.ir[t];
+        float f4, df4, f2, df2;
+        fcutf_d(P.d_rc4, r, f4, df4);
+        fcutf_d(P.d_rc2, r, f2, df2);
+        ws.fa[t] = f4;
+        ws.fb[t] = df4;
+#pragma unroll
+        for (int q = 0; q < BNE; q++) ws.P[t * BNE + q] = q < P.ne ? expf(-P.d_eta4[q] * r * r) : 0.0f;
+        int ds1 = (ws.sp[t] - s0 + ns) % ns;
+        const float *gg = ws.G + P.ind2[ds1];
+        float cp = 0.0f;
+        for (int f = 0; f < ng2; f++) {
+            float x = r - P.d_rs[f], eta = P.d_eta2[f];
+            cp += gg[f] * expf(-eta * x * x) * (-2.0f * eta * x * f2 + df2);
+        }
+        float cr = cp * ir;
+        float v0 = cr * d.x, v1 = cr * d.y, v2 = cr * d.z;
+        fi0 += v0; fi1 += v1; fi2 += v2;
+        ws.Fnb[3 * t] = -v0; ws.Fnb[3 * t + 1] = -v1; ws.Fnb[3 * t + 2] = -v2;
+        vr[0] -= (double)(v0 * d.x); vr[1] -= (double)(v1 * d.y); vr[2] -= (double)(v2 * d.z);
+        vr[3] -= (double)(v0 * d.y); vr[4] -= (double)(v1 * d.z); vr[5] -= (double)(v2 * d.x);
+        if (A.urep > 0.0) {
+            double R = P.rm[s0] + P.rm[ws.sp[t]], rd = (double)r;
+            if (rd < R) {
+                double sn, cs;
+                sincospi(rd / R, &sn, &cs);
+                double fu = 0.5 * (1.0 + cs), dfu = -0.5 * CUDART_PI / R * sn;
+                double tu = -2.0 * A.urep * R / (rd * rd) * (-fu / rd + dfu);
+                fi0 -= (float)(tu * d.x); fi1 -= (float)(tu * d.y); fi2 -= (float)(tu * d.z);
+                vr[0] += 0.5 * tu * d.x * d.x; vr[1] += 0.5 * tu * d.y * d.y; vr[2] += 0.5 * tu * d.z * d.z;
+                vr[3] += 0.5 * tu * d.x * d.y; vr[4] += 0.5 * tu * d.y * d.z; vr[5] += 0.5 * tu * d.z * d.x;
+            }
+        }
+    }
+    __syncwarp();
+
+    /* reverse triplets, reusing the lists when they fit */
+    blkid = 0;
+    for (int a = 0; a < ns; a++)
+        for (int b = a; b < ns; b++, blkid++) {
+            const int base = P.ind4[a * a + b * b];
+            for (int t = lane; t < BCELLS; t += 32) ws.grid[t] = 0.0f;
+            __syncwarp();
+            if (lane == 0)
+                for (int f = 0; f < P.ng4; f++) ws.grid[P.g4_cell[f]] += ws.G[base + f];
+            __syncwarp();
+            const int na = ws.seg[a], nb = ws.seg[b], oa = ws.seg[4 + a], ob = ws.seg[4 + b];
+            int row = 0, lo = whole ? ws.blk[blkid][0] : 0, hi = whole ? ws.blk[blkid][1] : 0;
+            for (;;) {
+                if (!whole) {
+                    hi = 0;
+                    for (; row < na; row++) {
+                        int jj = oa + row, k0 = (a == b) ? row + 1 : 0;
+                        if (hi + (nb - k0) > BTL) break;
+                        for (int kb = k0; kb < nb; kb += 32) {
+                            int kk = ob + kb + lane;
+                            bool ok = false;
+                            if (kb + lane < nb) ok = tgate(P, ws, s0, jj, kk);
+                            unsigned m = __ballot_sync(FULLM, ok);
+                            if (ok) ws.tl[hi + __popc(m & ((1u << lane) - 1u))] = (unsigned)jj | ((unsigned)kk << 16);
+                            hi += __popc(m);
+                        }
+                    }
+                    lo = 0;
+                    __syncwarp();
+                }
+                for (int t = lo + lane; t < hi; t += 32) {
+                    unsigned pk = ws.tl[t];
+                    int jj = pk & 0xffff, kk = pk >> 16;
+                    float4 d1 = ws.d[jj], d2 = ws.d[kk];
+                    float wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
+                    float r3s = wx * wx + wy * wy + wz * wz, r3 = sqrtf(r3s);
+                    if (!(d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq)) continue;
+                    float r1 = d1.w, r2 = d2.w, ir1 = ws.ir[jj], ir2 = ws.ir[kk], ir3 = 1.0f / r3;
+                    float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
+                    float f3, df3;
+                    fcutf_d(P.d_rc4, r3, f3, df3);
+                    float f1 = ws.fa[jj], df1 = ws.fb[jj], f2 = ws.fa[kk], df2 = ws.fb[kk];
+                    float lz[BNZL], lzp[BNZL];
+                    angularf(P, c, lz, lzp);
+                    float Q = 0.0f, Qe = 0.0f, Qc = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < BNE; q++) {
+                        float ex = ws.P[jj * BNE + q] * ws.P[kk * BNE + q] * expf(-P.d_eta4[q] * r3s);
+                        float u = 0.0f, vv = 0.0f;
+#pragma unroll
+                        for (int zl = 0; zl < BNZL; zl++) {
+                            float cg = ws.grid[q * BNZL + zl];
+                            u += cg * lz[zl];
+                            vv += cg * lzp[zl];
+                        }
+                        Q += ex * u;
+                        Qe += P.d_eta4[q] * ex * u;
+                        Qc += ex * vv;
+                    }
+                    float Af = 2.0f * f1 * f2 * f3;
+                    float T1 = 2.0f * df1 * f2 * f3 * Q - 2.0f * r1 * Af * Qe;
+                    float T2 = 2.0f * f1 * df2 * f3 * Q - 2.0f * r2 * Af * Qe;
+                    float T3 = 2.0f * f1 * f2 * df3 * Q - 2.0f * r3 * Af * Qe;
+                    float Tc = Af * Qc;
+                    float a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
+                    float a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
+                    float g1x = a11 * d1.x + a12 * d2.x - a3 * wx, g1y = a11 * d1.y + a12 * d2.y - a3 * wy,
+                          g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
+                    float g2x = a22 * d2.x + a12 * d1.x + a3 * wx, g2y = a22 * d2.y + a12 * d1.y + a3 * wy,
+                          g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                    fi0 += g1x + g2x; fi1 += g1y + g2y; fi2 += g1z + g2z;
+                    atomicAdd(&ws.Fnb[3 * jj], -g1x); atomicAdd(&ws.Fnb[3 * jj + 1], -g1y); atomicAdd(&ws.Fnb[3 * jj + 2], -g1z);
+                    atomicAdd(&ws.Fnb[3 * kk], -g2x); atomicAdd(&ws.Fnb[3 * kk + 1], -g2y); atomicAdd(&ws.Fnb[3 * kk + 2], -g2z);
+                    vr[0] -= (double)(g1x * d1.x + g2x * d2.x);
+                    vr[1] -= (double)(g1y * d1.y + g2y * d2.y);
+                    vr[2] -= (double)(g1z * d1.z + g2z * d2.z);
+                    vr[3] -= (double)(g1x * d1.y + g2x * d2.y);
+                    vr[4] -= (double)(g1y * d1.z + g2y * d2.z);
+                    vr[5] -= (double)(g1z * d1.x + g2z * d2.x);
+                }
+                __syncwarp();
+                if (whole || row >= na) break;
+            }
+        }
+    /* gather: atom i and its neighbours into the structure's force array */
+    fi0 = bsumf(fi0);
+    fi1 = bsumf(fi1);
+    fi2 = bsumf(fi2);
+    if (lane == 0) {
+        atomicAdd(&sh.F[3 * i], fi0);
+        atomicAdd(&sh.F[3 * i + 1], fi1);
+        atomicAdd(&sh.F[3 * i + 2], fi2);
+    }
+    for (int t = lane; t < n; t += 32) {
+        int j = ws.j[t];
+        atomicAdd(&sh.F[3 * j], ws.Fnb[3 * t]);
+        atomicAdd(&sh.F[3 * j + 1], ws.Fnb[3 * t + 1]);
+        atomicAdd(&sh.F[3 * j + 2], ws.Fnb[3 * t + 2]);
+    }
+#pragma unroll
+    for (int k = 0; k < 6; k++) virw[k] += bsum(vr[k]);
+    __syncwarp();
+}
+
+/* ---------------- one evaluation of the structure at DOF vector dof ---------------- */
+
+/* Returns H; gradient into gout; sh.scal[1] = max|F|, sh.scal[2] = max|U-pV|/N. */
+__device__ double evaluate(const BArgs &A, BShared &sh, const double *dof, double *gout) {
+    const BParams &P = *A.P;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, N = sh.N, rlxt = A.rlxt;
+    float4 *nbd = A.nbd + (size_t)blockIdx.x * BMAXN * BMAXNB;
+    int *nbj = A.nbj + (size_t)blockIdx.x * BMAXN * BMAXNB;
+    /* structure from the DOF vector (BUF_STR, src/cmin.c:54-88) */
+    if (tid == 0) {
+        if (rlxt != 2) {
+            const double *q = dof + 3 * N;
+            sh.L[0] = q[0]; sh.L[4] = q[1]; sh.L[8] = q[2]; sh.L[1] = q[3]; sh.L[5] = q[4];
+            sh.L[6] = q[5]; sh.L[3] = q[6]; sh.L[7] = q[7]; sh.L[2] = q[8];
+        }
+        reciprocal9(sh.L, sh.R);
+    }
+    __syncthreads();
+    for (int a = tid; a < N; a += blockDim.x) {
+        double f[3];
+        for (int q = 0; q < 3; q++) f[q] = dof[3 * a + q] - floor(dof[3 * a + q]);
+        for (int q = 0; q < 3; q++) sh.xc[3 * a + q] = f[0] * sh.L[q] + f[1] * sh.L[3 + q] + f[2] * sh.L[6 + q];
+        sh.F[3 * a] = sh.F[3 * a + 1] = sh.F[3 * a + 2] = 0.0f;
+    }
+    if (tid < 6) sh.uvir[tid] = 0.0;
+    __syncthreads();
+    /* neighbour lists: every (atom, image) within Rc, displacement in FP64 */
+    int nq[3];
+    for (int q = 0; q < 3; q++) {
+        double len = sqrt(sh.R[3 * q] * sh.R[3 * q] + sh.R[3 * q + 1] * sh.R[3 * q + 1] + sh.R[3 * q + 2] * sh.R[3 * q + 2]);
+        nq[q] = (int)ceil(P.rc * len);
+    }
+    const int w0 = 2 * nq[0] + 1, w1 = 2 * nq[1] + 1, w2 = 2 * nq[2] + 1, nimg = w0 * w1 * w2;
+    const double rc2 = P.rc * P.rc;
+    for (int i = w; i < N; i += BWARPS) {
+        int count = 0;
+        const double xi0 = sh.xc[3 * i], xi1 = sh.xc[3 * i + 1], xi2 = sh.xc[3 * i + 2];
+        for (int base = 0; base < N * nimg; base += 32) {
+            int cidx = base + lane;
+            bool ok = false;
+            double d0 = 0, d1 = 0, d2 = 0, r2 = 0;
+            int j = 0;
+            if (cidx < N * nimg) {
+                j = cidx / nimg;
+                int im = cidx % nimg, c2 = im % w2 - nq[2], t = im / w2, c1 = t % w1 - nq[1], c0 = t / w1 - nq[0];
+                if (!(j == i && c0 == 0 && c1 == 0 && c2 == 0)) {
+                    d0 = c0 * sh.L[0] + c1 * sh.L[3] + c2 * sh.L[6] + sh.xc[3 * j] - xi0;
+                    d1 = c0 * sh.L[1] + c1 * sh.L[4] + c2 * sh.L[7] + sh.xc[3 * j + 1] - xi1;
+                    d2 = c0 * sh.L[2] + c1 * sh.L[5] + c2 * sh.L[8] + sh.xc[3 * j + 2] - xi2;
+                    r2 = d0 * d0 + d1 * d1 + d2 * d2;
+                    ok = r2 < rc2;
+                }
+            }
+            unsigned m = __ballot_sync(FULLM, ok);
+            int pos = count + __popc(m & ((1u << lane) - 1u));
+            if (ok && pos < BMAXNB) {
+                nbj[i * BMAXNB + pos] = j;
+                nbd[i * BMAXNB + pos] = make_float4((float)d0, (float)d1, (float)d2, (float)sqrt(r2));
+            }
+            count += __popc(m);
+        }
+        if (lane == 0) {
+            sh.nn[i] = count < BMAXNB ? count : BMAXNB;
+            if (count > BMAXNB) sh.flag = 2;
+        }
+    }
+    __syncthreads();
+    /* descriptors, MLP and forces, one warp per atom */
+    double virw[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = w; i < N; i += BWARPS) atom_pass(A, sh, sh.ws[w], i, nbd, nbj, virw);
+    if (lane == 0)
+        for (int k = 0; k < 6; k++) sh.vir[w][k] = virw[k];
+    __syncthreads();
+    /* FP64 reductions, enthalpy and the DOF gradient (cdfunc_gsl, src/cmin.c:107-166) */
+    if (tid == 0) {
+        double E = 0.0, U[6];
+        for (int a = 0; a < N; a++) E += sh.ea[a] + sh.eu[a];
+        for (int k = 0; k < 6; k++) {
+            U[k] = 0.0;
+            for (int ww = 0; ww < BWARPS; ww++) U[k] += sh.vir[ww][k];
+        }
+        const double *L = sh.L;
+        double V = fabs(L[0] * L[4] * L[8] + L[2] * L[3] * L[7] + L[1] * L[5] * L[6] - L[0] * L[5] * L[7] -
+                        L[1] * L[3] * L[8] - L[2] * L[4] * L[6]);
+        double pv = A.p_ev * V;
+        sh.scal[0] = E + pv;
+        for (int q = 0; q < 3; q++) U[q] -= pv;
+        for (int k = 0; k < 6; k++) sh.uvir[k] = U[k];
+        double mu = 0.0;
+        if (rlxt != 2)
+            for (int k = 0; k < 6; k++) mu = fmax(mu, fabs(U[k]) / N);
+        sh.scal[2] = mu;
+    }
+    __syncthreads();
+    double mf = 0.0;
+    for (int a = tid; a < N; a += blockDim.x)
+        for (int q = 0; q < 3; q++) {
+            double gq = 0.0;
+            for (int k = 0; k < 3; k++) gq -= (double)sh.F[3 * a + k] * sh.L[3 * q + k];
+            gout[3 * a + q] = fabs(gq) < 1e-10 ? 0.0 : gq;
+            mf = fmax(mf, fabs((double)sh.F[3 * a + q]));
+        }
+    mf = cta_max(sh, mf);
+    if (tid == 0) {
+        sh.scal[1] = mf;
+        if (rlxt != 2) {
+            const double *U = sh.uvir, *R = sh.R;
+            double *q = gout + 3 * N;
+            q[0] = -(U[0] * R[0] + U[3] * R[1] + U[5] * R[2]);
+            q[1] = -(U[3] * R[3] + U[1] * R[4] + U[4] * R[5]);
+            q[2] = -(U[5] * R[6] + U[4] * R[7] + U[2] * R[8]);
+            q[3] = -(U[3] * R[0] + U[1] * R[1] + U[4] * R[2]);
+            q[4] = -(U[5] * R[3] + U[4] * R[4] + U[2] * R[5]);
+            q[5] = -(U[0] * R[6] + U[3] * R[7] + U[5] * R[8]);
+            q[6] = -(U[0] * R[3] + U[3] * R[4] + U[5] * R[5]);
+            q[7] = -(U[3] * R[6] + U[1] * R[7] + U[4] * R[8]);
+            q[8] = -(U[5] * R[0] + U[4] * R[1] + U[2] * R[2]);
+            for (int k = 0; k < 9; k++)
+                if (fabs(q[k]) < 1e-10) q[k] = 0.0;
+        }
+        atomicAdd((unsigned long long *)A.evals, 1ull);
+    }
+    __syncthreads();
+    return sh.scal[0];
+}
+
+/* cubic (or quadratic without db) minimiser on [lo,hi] (Fletcher, sec. 2.6) */
+__device__ double interp_min(double a, double fa, double da, double b, double fb, double db, double lo, double hi) {
+    double w = b - a;
+    if (w == 0.0) return a;
+    double zlo = (lo - a) / w, zhi = (hi - a) / w;
+    if (zlo > zhi) { double t = zlo; zlo = zhi; zhi = t; }
+    double c0 = fa, c1 = da * w, c2 = 3.0 * (fb - fa) - 2.0 * c1 - db * w, c3 = c1 + db * w - 2.0 * (fb - fa);
+    double cand[4];
+    int nc = 0;
+    cand[nc++] = zlo;
+    cand[nc++] = zhi;
+    if (c3 != 0.0) {
+        double disc = 4.0 * c2 * c2 - 12.0 * c3 * c1;
+        if (disc >= 0.0) {
+            double sq = sqrt(disc), q = -0.5 * (2.0 * c2 + (c2 >= 0.0 ? sq : -sq));
+            if (q != 0.0) {
+                cand[nc++] = q / (3.0 * c3);
+                cand[nc++] = c1 / q;
+            }
+        }
+    } else if (c2 > 0.0) {
+        cand[nc++] = -c1 / (2.0 * c2);
+    }
+    double best = zlo, fbest = 1e300;
+    for (int k = 0; k < nc; k++) {
+        double z = cand[k];
+        if (!(z >= zlo && z <= zhi)) continue;
+        double fz = c0 + z * (c1 + z * (c2 + z * c3));
+        if (fz < fbest) { fbest = fz; best = z; }
+    }
+    return a + best * w;
+}
+
+__device__ void vcopy(double *dst, const double *src, int n) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
+}
+
+__global__ void __launch_bounds__(BWARPS * 32) k_relax_batch(BArgs A) {
+    extern __shared__ __align__(16) char smem_raw[];
+    BShared &sh = *reinterpret_cast<BShared *>(smem_raw);
+    const int tid = threadIdx.x;
+    double *H = A.hmat + (size_t)blockIdx.x * BMAXDOF * BMAXDOF;
+    const double rho = 0.01, tau1 = 9.0, tau2 = 0.05, tau3 = 0.5;
+    for (;;) {
+        if (tid == 0) sh.s = atomicAdd(A.queue, 1);
+        __syncthreads();
+        const int s = sh.s;
+        if (s >= A.S) break;
+        const int N = A.nat[s], o = A.off[s], rlxt = A.rlxt;
+        const int n = 3 * N + (rlxt == 3 ? 9 : 0);
+        if (tid == 0) {
+            sh.N = N;
+            sh.ndof = n;
+            sh.flag = 0;
+            for (int k = 0; k < 9; k++) sh.L[k] = A.lat[9 * s + k];
+            reciprocal9(sh.L, sh.R);
+        }
+        __syncthreads();
+        /* DOF vector: fractional coordinates then lattice (STR_BUF, src/cmin.c:22-52) */
+        for (int a = tid; a < N; a += blockDim.x) {
+            sh.spc[a] = A.spc[o + a];
+            for (int q = 0; q < 3; q++) {
+                const double *xa = A.x + 3 * (size_t)(o + a);
+                sh.x[3 * a + q] = xa[0] * sh.R[3 * q] + xa[1] * sh.R[3 * q + 1] + xa[2] * sh.R[3 * q + 2];
+            }
+        }
+        if (tid == 0 && rlxt == 3) {
+            double *q = sh.x + 3 * N;
+            q[0] = sh.L[0]; q[1] = sh.L[4]; q[2] = sh.L[8]; q[3] = sh.L[1]; q[4] = sh.L[5];
+            q[5] = sh.L[6]; q[6] = sh.L[3]; q[7] = sh.L[7]; q[8] = sh.L[2];
+        }
+        for (int k = tid; k < n * n; k += blockDim.x) H[k] = (k / n == k % n) ? 1.0 : 0.0;
+        __syncthreads();
+        double f = evaluate(A, sh, sh.x, sh.g), fprev = f;
+        double maxf = sh.scal[1], maxu = sh.scal[2];
+        int first = 1, iter = 0, status = 1;
+        if (sh.flag) status = 2;
+        else if (maxf < A.fmax && maxu < A.fmax) status = 0;
+        while (status == 1 && iter < A.mitr) {
+            iter++;
+            /* p = -H g */
+            for (int r = tid; r < n; r += blockDim.x) {
+                double t = 0.0;
+                for (int c = 0; c < n; c++) t += H[r * n + c] * sh.g[c];
+                sh.p[r] = -t;
+            }
+            __syncthreads();
+            double dphi0 = 0.0, pp = 0.0;
+            for (int k = tid; k < n; k += blockDim.x) { dphi0 += sh.g[k] * sh.p[k]; }
+            dphi0 = cta_sum(sh, dphi0);
+            if (!(dphi0 < 0.0)) {
+                for (int k = tid; k < n * n; k += blockDim.x) H[k] = (k / n == k % n) ? 1.0 : 0.0;
+                for (int k = tid; k < n; k += blockDim.x) sh.p[k] = -sh.g[k];
+                __syncthreads();
+                first = 1;
+                dphi0 = 0.0;
+                for (int k = tid; k < n; k += blockDim.x) dphi0 += sh.g[k] * sh.p[k];
+                dphi0 = cta_sum(sh, dphi0);
+                if (!(dphi0 < 0.0)) { status = 0; break; } /* zero gradient: at a stationary point */
+            }
+            for (int k = tid; k < n; k += blockDim.x) pp += sh.p[k] * sh.p[k];
+            pp = cta_sum(sh, pp);
+            double alpha = first ? 0.01 / sqrt(pp) : 2.0 * (f - fprev) / dphi0;
+            if (!first && (!(alpha > 0.0) || alpha > 1.0)) alpha = 1.0;
+            /* Fletcher line search with energy and gradient at every trial */
+            double ap = 0.0, fp = f, dp = dphi0, a = 0, fa = 0, da = 0, b = 0, fb = 0, db = 0;
+            double a_maxf = maxf, a_maxu = maxu, ft = 0.0, dt;
+            int phase = 0, done = 0, trial;
+            vcopy(sh.xa, sh.x, n);
+            vcopy(sh.ga, sh.g, n);
+            __syncthreads();
+            for (trial = 0; trial < 60 && !done; trial++) {
+                for (int k = tid; k < n; k += blockDim.x) sh.xt[k] = sh.x[k] + alpha * sh.p[k];
+                __syncthreads();
+                ft = evaluate(A, sh, sh.xt, sh.gt);
+                double t = 0.0;
+                for (int k = tid; k < n; k += blockDim.x) t += sh.gt[k] * sh.p[k];
+                dt = cta_sum(sh, t);
+                if (sh.flag) { done = 3; break; }
+                const double mft = sh.scal[1], mut = sh.scal[2];
+                int save_a = 0;
+                double next = alpha;
+                if (!isfinite(ft)) { done = 4; break; }
+                if (phase == 0) {
+                    if (ft > f + rho * alpha * dphi0 || (trial > 0 && ft >= fp)) {
+                        a = ap; fa = fp; da = dp; b = alpha; fb = ft; db = dt;
+                        phase = 1;
+                    } else if (fabs(dt) <= -A.sigma * dphi0) {
+                        done = 1;
+                    } else if (dt >= 0.0) {
+                        a = alpha; fa = ft; da = dt; b = ap; fb = fp; db = dp;
+                        save_a = 1;
+                        phase = 1;
+                    } else {
+                        next = interp_min(ap, fp, dp, alpha, ft, dt, 2.0 * alpha - ap, alpha + tau1 * (alpha - ap));
+                        ap = alpha; fp = ft; dp = dt;
+                        save_a = 1;
+                    }
+                } else {
+                    if (ft > f + rho * alpha * dphi0 || ft >= fa) {
+                        b = alpha; fb = ft; db = dt;
+                    } else if (fabs(dt) <= -A.sigma * dphi0) {
+                        done = 1;
+                    } else {
+                        if ((b - a) * dt >= 0.0) { b = a; fb = fa; db = da; }
+                        a = alpha; fa = ft; da = dt;
+                        save_a = 1;
+                    }
+                }
+                if (save_a) {
+                    vcopy(sh.xa, sh.xt, n);
+                    vcopy(sh.ga, sh.gt, n);
+                    a_maxf = mft;
+                    a_maxu = mut;
+                }
+                if (done) {
+                    maxf = mft;
+                    maxu = mut;
+                    break;
+                }
+                if (phase == 1) {
+                    if (fabs((a - b) * da) <= 4.0 * 2.220446049250313e-16 * (fabs(f) + 1.0) || trial == 59) {
+                        done = 2; /* interval exhausted: the best point stands */
+                        break;
+                    }
+                    next = interp_min(a, fa, da, b, fb, db, a + tau2 * (b - a), b - tau3 * (b - a));
+                }
+                alpha = next;
+                __syncthreads();
+            }
+            __syncthreads();
+            if (done == 3) { status = 2; break; }
+            if (done == 2 || done == 4 || done == 0) {
+                /* accept the best bracketed point if it lowered the enthalpy */
+                if (phase == 1 && a > 0.0 && fa < f) {
+                    vcopy(sh.xt, sh.xa, n);
+                    vcopy(sh.gt, sh.ga, n);
+                    alpha = a;
+                    ft = fa;
+                    maxf = a_maxf;
+                    maxu = a_maxu;
+                    __syncthreads();
+                } else {
+                    status = 3;
+                    break;
+                }
+            }
+            /* BFGS update with s = alpha p, y = gt - g (Nocedal & Wright 6.17, 6.20) */
+            for (int k = tid; k < n; k += blockDim.x) {
+                sh.p[k] *= alpha;
+                sh.hy[k] = sh.gt[k] - sh.g[k];
+            }
+            __syncthreads();
+            double sy = 0.0, yy = 0.0;
+            for (int k = tid; k < n; k += blockDim.x) { sy += sh.p[k] * sh.hy[k]; yy += sh.hy[k] * sh.hy[k]; }
+            sy = cta_sum(sh, sy);
+            yy = cta_sum(sh, yy);
+            if (sy > 0.0) {
+                if (first)
+                    for (int k = tid; k < n * n; k += blockDim.x) H[k] = (k / n == k % n) ? sy / yy : 0.0;
+                __syncthreads();
+                /* Hy into g (g is replaced below) */
+                for (int r = tid; r < n; r += blockDim.x) {
+                    double t = 0.0;
+                    for (int c = 0; c < n; c++) t += H[r * n + c] * sh.hy[c];
+                    sh.g[r] = t;
+                }
+                __syncthreads();
+                double yhy = 0.0;
+                for (int k = tid; k < n; k += blockDim.x) yhy += sh.hy[k] * sh.g[k];
+                yhy = cta_sum(sh, yhy);
+                const double c1 = (sy + yhy) / (sy * sy);
+                for (int k = tid; k < n * n; k += blockDim.x) {
+                    int r = k / n, c = k % n;
+                    H[k] += c1 * sh.p[r] * sh.p[c] - (sh.g[r] * sh.p[c] + sh.p[r] * sh.g[c]) / sy;
+                }
+            }
+            __syncthreads();
+            vcopy(sh.x, sh.xt, n);
+            vcopy(sh.g, sh.gt, n);
+            __syncthreads();
+            fprev = f;
+            f = ft;
+            first = 0;
+            if (maxf < A.fmax && maxu < A.fmax) status = 0;
+        }
+        /* results: Cartesian positions of the final DOF vector */
+        if (tid == 0) {
+            if (rlxt == 3) {
+                const double *q = sh.x + 3 * N;
+                sh.L[0] = q[0]; sh.L[4] = q[1]; sh.L[8] = q[2]; sh.L[1] = q[3]; sh.L[5] = q[4];
+                sh.L[6] = q[5]; sh.L[3] = q[6]; sh.L[7] = q[7]; sh.L[2] = q[8];
+            }
+            for (int k = 0; k < 9; k++) A.lat[9 * s + k] = sh.L[k];
+            A.H[s] = f;
+            A.iters[s] = iter;
+            A.status[s] = status;
+        }
+        __syncthreads();
+        for (int a = tid; a < N; a += blockDim.x)
+            for (int q = 0; q < 3; q++)
+                A.x[3 * (size_t)(o + a) + q] = sh.x[3 * a] * sh.L[q] + sh.x[3 * a + 1] * sh.L[3 + q] + sh.x[3 * a + 2] * sh.L[6 + q];
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+/* ---------------- host launcher ---------------- */
+
+static int build_bparams(const mb_model *m, BParams *B, float **w_out, size_t *wlen) {
+    const mb_params &P = m->P;
+    memset(B, 0, sizeof(*B));
+    if (P.ne > BNE || P.nz > BNZ || P.nlam > BNLAM || P.D > BMAXD || P.ng2 > 16) return -1;
+    B->nspc = P.nspc; B->D = P.D; B->ng2 = P.ng2; B->ng4 = P.ng4; B->ne = P.ne; B->nz = P.nz; B->nlam = P.nlam;
+    B->h1 = P.h1; B->h2 = P.h2;
+    memcpy(B->ind2, P.ind2, sizeof(B->ind2));
+    memcpy(B->ind4, P.ind4, sizeof(B->ind4));
+    for (int p = 0; p < MB_NPAIR; p++) {
+        B->f_rc2[p] = (float)P.f_rc2[p];
+        B->f_rc4[p] = (float)P.f_rc4[p];
+        B->f_rc4sq[p] = (float)P.f_rc4sq[p];
+        for (int f = 0; f < MB_MAXG2; f++) {
+            B->f_eta2[p][f] = (float)P.f_eta2[p][f];
+            B->f_rs[p][f] = (float)P.f_rs[p][f];
+        }
+        for (int e = 0; e < MB_MAXE; e++) B->f_eta4[p][e] = (float)P.f_eta4[p][e];
+    }
+    B->d_rc2 = (float)P.d_rc2; B->d_rc4 = (float)P.d_rc4; B->d_rc4sq = (float)P.d_rc4sq;
+    for (int f = 0; f < MB_MAXG2; f++) {
+        B->d_eta2[f] = (float)P.d_eta2[f];
+        B->d_rs[f] = (float)P.d_rs[f];
+    }
+    for (int e = 0; e < MB_MAXE; e++) B->d_eta4[e] = (float)P.d_eta4[e];
+    if (!P.zeta_int) return -1;
+    for (int z = 0; z < MB_MAXZ; z++) {
+        B->zeta[z] = (float)P.zeta[z];
+        B->powz[z] = (float)P.powz[z];
+        B->zbits[z] = z < P.nz ? P.zbits[z] : 0;
+        B->zm1bits[z] = z < P.nz ? P.zm1bits[z] : 0;
+    }
+    for (int l = 0; l < MB_MAXL; l++) B->lam[l] = (float)P.lam[l];
+    for (int f = 0; f < P.ng4; f++) B->g4_cell[f] = P.g4_e[f] * BNZL + (P.g4_zl[f] / P.nlam) * BNLAM + P.g4_zl[f] % P.nlam;
+    for (int s = 0; s < MB_MAXSPC; s++) {
+        B->rm[s] = P.rm[s];
+        B->w_off[s] = P.w_off[s];
+    }
+    B->rc = m->rc_list;
+    *wlen = m->weights_len;
+    float *w = (float *)malloc(sizeof(float) * m->weights_len);
+    for (size_t k = 0; k < m->weights_len; k++) w[k] = (float)m->weights[k];
+    *w_out = w;
+    return 0;
+}
+
+extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const int *d_off, const int *d_spc,
+                               double *d_lat, double *d_x, double p_ev, double urep, int rlxt, int mitr, double fmax,
+                               double *d_H, int *d_iters, int *d_status, void *stream, long long *evals_out,
+                               float *ms_out) {
+    cudaStream_t st = (cudaStream_t)stream;
+    BParams hp;
+    float *hw = nullptr;
+    size_t wlen = 0;
+    if (build_bparams(m, &hp, &hw, &wlen)) return (int)cudaErrorInvalidValue;
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t smem = sizeof(BShared);
+    cudaError_t e = cudaFuncSetAttribute(k_relax_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) { free(hw); return (int)e; }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_batch, BWARPS * 32, smem);
+    if (per < 1) { free(hw); return (int)cudaErrorInvalidConfiguration; }
+    int grid = sms * per < S ? sms * per : S;
+    BParams *dp = nullptr;
+    float *dw = nullptr;
+    double *hm = nullptr;
+    float4 *nbd = nullptr;
+    int *nbj = nullptr, *queue = nullptr;
+    long long *evals = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    e = cudaMalloc(&dp, sizeof(BParams));
+    if (!e) e = cudaMalloc(&dw, sizeof(float) * wlen);
+    if (!e) e = cudaMalloc(&hm, sizeof(double) * (size_t)grid * BMAXDOF * BMAXDOF);
+    if (!e) e = cudaMalloc(&nbd, sizeof(float4) * (size_t)grid * BMAXN * BMAXNB);
+    if (!e) e = cudaMalloc(&nbj, sizeof(int) * (size_t)grid * BMAXN * BMAXNB);
+    if (!e) e = cudaMalloc(&queue, sizeof(int));
+    if (!e) e = cudaMalloc(&evals, sizeof(long long));
+    if (!e) e = cudaMemcpyAsync(dp, &hp, sizeof(BParams), cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaMemcpyAsync(dw, hw, sizeof(float) * wlen, cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaMemsetAsync(queue, 0, sizeof(int), st);
+    if (!e) e = cudaMemsetAsync(evals, 0, sizeof(long long), st);
+    if (!e) {
+        BArgs a;
+        a.S = S; a.rlxt = rlxt; a.mitr = mitr;
+        a.p_ev = p_ev; a.urep = urep; a.fmax = fmax; a.sigma = 0.1;
+        a.nat = d_nat; a.off = d_off; a.spc = d_spc;
+        a.lat = d_lat; a.x = d_x; a.H = d_H; a.iters = d_iters; a.status = d_status;
+        a.P = dp; a.W = dw; a.queue = queue; a.hmat = hm; a.nbd = nbd; a.nbj = nbj; a.evals = evals;
+        cudaEventRecord(e0, st);
+        k_relax_batch<<<grid, BWARPS * 32, smem, st>>>(a);
+        cudaEventRecord(e1, st);
+        e = cudaGetLastError();
+    }
+    if (!e) e = cudaStreamSynchronize(st);
+    if (!e && evals_out) e = cudaMemcpy(evals_out, evals, sizeof(long long), cudaMemcpyDeviceToHost);
+    if (!e && ms_out) cudaEventElapsedTime(ms_out, e0, e1);
+    cudaFree(dp); cudaFree(dw); cudaFree(hm); cudaFree(nbd); cudaFree(nbj); cudaFree(queue); cudaFree(evals);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    free(hw);
+    return (int)e;
+}

@@ -280,6 +280,25 @@ __device__ __forceinline__ void fcut_d(double rc, double r, double &f, double &d
  * upper bounds (exact for the specialised kernels); zl = z*NLAM + l. */
 template <int NZ, int NLAM>
 __device__ __forceinline__ void angular(const mb_params &P, double c, double *lz, double *lzp) {
+    if (NZ == 4 && P.zeta_std) {
+        /* zeta = 1, 2, 4, 16 (the reference bases): powers by squaring */
+#pragma unroll
+        for (int l = 0; l < NLAM; l++) {
+            if (l >= P.nlam) break;
+            const double lam = P.lam[l], b1 = 1.0 + lam * c, b2 = b1 * b1, b4 = b2 * b2, b8 = b4 * b4;
+            lz[0 * NLAM + l] = P.powz[0] * b1;
+            lz[1 * NLAM + l] = P.powz[1] * b2;
+            lz[2 * NLAM + l] = P.powz[2] * b4;
+            lz[3 * NLAM + l] = P.powz[3] * (b8 * b8);
+            if (lzp) {
+                lzp[0 * NLAM + l] = P.powz[0] * lam;
+                lzp[1 * NLAM + l] = P.powz[1] * 2.0 * lam * b1;
+                lzp[2 * NLAM + l] = P.powz[2] * 4.0 * lam * (b2 * b1);
+                lzp[3 * NLAM + l] = P.powz[3] * 16.0 * lam * (b8 * b4 * b2 * b1);
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int l = 0; l < NLAM; l++) {
         if (l >= P.nlam) break;
@@ -505,7 +524,14 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
     constexpr int NZL = NZ * NLAM;
     constexpr int WARPS = WPA;
     extern __shared__ __align__(16) char smem_raw[];
-    const mb_params &P = *A.params;
+    __shared__ mb_params Ps;
+    {
+        const int *src = reinterpret_cast<const int *>(A.params);
+        int *dst = reinterpret_cast<int *>(&Ps);
+        for (int k = threadIdx.x; k < (int)(sizeof(mb_params) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+        __syncthreads();
+    }
+    const mb_params &P = Ps;
     const int NT = WPA * 32, group = threadIdx.x / NT;
     const int tid = threadIdx.x % NT, lane = threadIdx.x & 31, warp = tid >> 5;
     const int i = blockIdx.x * APB + group;

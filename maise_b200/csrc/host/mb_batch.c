@@ -1,0 +1,94 @@
+/*
+ * mb_batch.c -- host side of the population relax: packs the structures,
+ * launches the persistent kernel (mb_batch.cu) and returns the results.
+ */
+#include <cuda_runtime_api.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../../../include/maise_b200.h"
+#include "mb_batch.h"
+
+#define MB_EV2GPA 160.2176565 /* src/util.c:8 */
+
+/* the handle layout is private to mb_core.c; these accessors are defined there */
+const mb_model *mb_handle_model(const mb_potential *p);
+void *mb_handle_stream(mb_potential *p);
+int mb_handle_device(const mb_potential *p);
+int mb_handle_fail(int code, const char *msg);
+void mb_handle_set_batch_stats(mb_potential *p, long long evals, float ms);
+
+int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, double *lat, double *x, double p_gpa,
+                   double urep, int rlxt, int mitr, double fmax, double *H, int *iters, int *status) {
+    int *off, total = 0, s, rc = MB_OK;
+    int *d_nat = NULL, *d_off = NULL, *d_spc = NULL, *d_iters = NULL, *d_status = NULL;
+    double *d_lat = NULL, *d_x = NULL, *d_H = NULL;
+    long long evals = 0;
+    float ms = 0.0f;
+    const mb_model *m;
+    void *st;
+    cudaError_t e;
+    if (!pot || S < 1 || !nat || !atmn || !lat || !x || !H || !iters || !status || !(fmax > 0) || mitr < 0)
+        return mb_handle_fail(MB_ERR_ARG, "bad arguments");
+    if (!(rlxt == 2 || rlxt == 3)) return mb_handle_fail(MB_ERR_ARG, "batched relax supports RLXT 2 and 3");
+    m = mb_handle_model(pot);
+    off = (int *)malloc(sizeof(int) * (S + 1));
+    for (s = 0; s < S; s++) {
+        if (nat[s] < 1 || nat[s] > 64) {
+            free(off);
+            return mb_handle_fail(MB_ERR_ARG, "batched relax takes 1..64 atoms per structure");
+        }
+        off[s] = total;
+        total += nat[s];
+    }
+    off[S] = total;
+    for (s = 0; s < total; s++)
+        if (atmn[s] < 0 || atmn[s] >= m->nspc) {
+            free(off);
+            return mb_handle_fail(MB_ERR_ARG, "species index out of range");
+        }
+    cudaSetDevice(mb_handle_device(pot));
+    st = mb_handle_stream(pot);
+    e = cudaMalloc((void **)&d_nat, sizeof(int) * S);
+    if (!e) e = cudaMalloc((void **)&d_off, sizeof(int) * (S + 1));
+    if (!e) e = cudaMalloc((void **)&d_spc, sizeof(int) * total);
+    if (!e) e = cudaMalloc((void **)&d_iters, sizeof(int) * S);
+    if (!e) e = cudaMalloc((void **)&d_status, sizeof(int) * S);
+    if (!e) e = cudaMalloc((void **)&d_lat, sizeof(double) * 9 * S);
+    if (!e) e = cudaMalloc((void **)&d_x, sizeof(double) * 3 * total);
+    if (!e) e = cudaMalloc((void **)&d_H, sizeof(double) * S);
+    if (!e) e = cudaMemcpyAsync(d_nat, nat, sizeof(int) * S, cudaMemcpyHostToDevice, (cudaStream_t)st);
+    if (!e) e = cudaMemcpyAsync(d_off, off, sizeof(int) * (S + 1), cudaMemcpyHostToDevice, (cudaStream_t)st);
+    if (!e) e = cudaMemcpyAsync(d_spc, atmn, sizeof(int) * total, cudaMemcpyHostToDevice, (cudaStream_t)st);
+    if (!e) e = cudaMemcpyAsync(d_lat, lat, sizeof(double) * 9 * S, cudaMemcpyHostToDevice, (cudaStream_t)st);
+    if (!e) e = cudaMemcpyAsync(d_x, x, sizeof(double) * 3 * total, cudaMemcpyHostToDevice, (cudaStream_t)st);
+    if (e) {
+        rc = mb_handle_fail(MB_ERR_CUDA, cudaGetErrorString(e));
+        goto out;
+    }
+    e = (cudaError_t)mbk_relax_batch(m, S, d_nat, d_off, d_spc, d_lat, d_x, p_gpa / MB_EV2GPA, urep > 0 ? urep : 0.0,
+                                     rlxt, mitr, fmax, d_H, d_iters, d_status, st, &evals, &ms);
+    if (e == cudaErrorInvalidValue) {
+        rc = mb_handle_fail(MB_ERR_MODEL, "batched relax needs a basis with <= 7 G4 exponents, zeta in {integers}, "
+                                          "2 lambdas, <= 16 G2 functions and D <= 288");
+        goto out;
+    }
+    if (e) {
+        rc = mb_handle_fail(MB_ERR_CUDA, cudaGetErrorString(e));
+        goto out;
+    }
+    e = cudaMemcpy(lat, d_lat, sizeof(double) * 9 * S, cudaMemcpyDeviceToHost);
+    if (!e) e = cudaMemcpy(x, d_x, sizeof(double) * 3 * total, cudaMemcpyDeviceToHost);
+    if (!e) e = cudaMemcpy(H, d_H, sizeof(double) * S, cudaMemcpyDeviceToHost);
+    if (!e) e = cudaMemcpy(iters, d_iters, sizeof(int) * S, cudaMemcpyDeviceToHost);
+    if (!e) e = cudaMemcpy(status, d_status, sizeof(int) * S, cudaMemcpyDeviceToHost);
+    if (e) rc = mb_handle_fail(MB_ERR_CUDA, cudaGetErrorString(e));
+    mb_handle_set_batch_stats(pot, evals, ms);
+out:
+    cudaFree(d_nat); cudaFree(d_off); cudaFree(d_spc); cudaFree(d_iters); cudaFree(d_status);
+    cudaFree(d_lat); cudaFree(d_x); cudaFree(d_H);
+    free(off);
+    return rc;
+}

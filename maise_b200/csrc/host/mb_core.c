@@ -25,6 +25,8 @@
 struct mb_potential {
     mb_model m;
     int device;
+    long long batch_evals;
+    float batch_ms;
     cudaStream_t stream;
     mb_dev d;
     long launches;
@@ -155,6 +157,23 @@ int mb_model_info(const mb_potential *p, int *nspc, int *spcz, int *D, double *r
 }
 
 void *mb_stream(mb_potential *p) { return p ? (void *)p->stream : NULL; }
+
+/* accessors for the other host files (mb_batch.c) */
+const mb_model *mb_handle_model(const mb_potential *p) { return &p->m; }
+void *mb_handle_stream(mb_potential *p) { return (void *)p->stream; }
+int mb_handle_device(const mb_potential *p) { return p->device; }
+int mb_handle_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+void mb_handle_set_batch_stats(mb_potential *p, long long evals, float ms) {
+    p->batch_evals = evals;
+    p->batch_ms = ms;
+}
+
+int mb_batch_stats(const mb_potential *p, long long *evals, double *ms) {
+    if (!p) return fail(MB_ERR_ARG, "null handle");
+    if (evals) *evals = p->batch_evals;
+    if (ms) *ms = p->batch_ms;
+    return MB_OK;
+}
 
 int mb_profile(mb_potential *p, int enable, int capacity) {
     mb_dev *d;
@@ -518,6 +537,10 @@ typedef struct {
     double p_gpa, urep, H;
     int err;
     long ne, nf;
+    /* force criterion of the last energy+gradient evaluation and its DOF */
+    double maxf, maxu;
+    double *last_x;
+    int ndof;
 } relax_ctx;
 
 /* STR_BUF: DOF vector from the current structure (src/cmin.c:22-52) */
@@ -604,15 +627,83 @@ static double relax_eval(relax_ctx *r, double *x, double *g) {
         }
         for (i = 0; i < j; i++)
             if (fabs(g[i]) < 1e-10) g[i] = 0.0;
+        /* force criterion at this point: max |F| and max |U - pV| / N */
+        {
+            double mf = 0.0, mu = 0.0, pv = r->p_gpa / MB_EV2GPA * V;
+            for (i = 0; i < 3 * r->N; i++)
+                if (fabs(r->F[i]) > mf) mf = fabs(r->F[i]);
+            for (q = 0; q < 6; q++) {
+                double u = (r->rlxt == 2) ? 0.0 : fabs(U[q]) / r->N;
+                if (u > mu) mu = u;
+            }
+            (void)pv;
+            r->maxf = mf;
+            r->maxu = mu;
+        }
     }
     /* STR_BUF after the wrap performed by the list build */
     cart_to_frac(r->N, r->xc, r->L, r->xf);
     str_buf(r, x);
+    if (g && r->last_x) memcpy(r->last_x, x, sizeof(double) * r->ndof);
     return r->H;
 }
 
 static double relax_f(void *ctx, double *x) { return relax_eval((relax_ctx *)ctx, x, NULL); }
 static double relax_fg(void *ctx, double *x, double *g) { return relax_eval((relax_ctx *)ctx, x, g); }
+
+/* Relaxation with the force criterion (see mb_relax_fmax): the same DOF
+ * mapping and BFGS, line-search tolerance 0.1. */
+int mb_relax_fmax(mb_potential *p, int N, int NM, int ND, const int *atmn, double *lat9, double *x, double p_gpa,
+                  double urep, int rlxt, int mitr, double fmax, double *H, long *counts, int *converged) {
+    relax_ctx r;
+    mb_bfgs b;
+    double *dof, *gtmp;
+    int n, iter = 0, rc = MB_OK, st, conv = 0;
+    if (!p || N < 1 || !atmn || !lat9 || !x || !(fmax > 0)) return fail(MB_ERR_ARG, "bad arguments");
+    if (!(rlxt == 2 || rlxt == 3)) return fail(MB_ERR_ARG, "RLXT %d not supported here (2, 3)", rlxt);
+    memset(&r, 0, sizeof(r));
+    r.p = p; r.N = N; r.NM = NM; r.ND = ND; r.rlxt = rlxt; r.atmn = atmn; r.p_gpa = p_gpa; r.urep = urep;
+    memcpy(r.L, lat9, sizeof(double) * 9);
+    n = 3 * N + (rlxt == 3 ? 9 : 0);
+    r.ndof = n;
+    r.xf = (double *)malloc(sizeof(double) * 3 * N);
+    r.xc = (double *)malloc(sizeof(double) * 3 * N);
+    r.F = (double *)malloc(sizeof(double) * 3 * N);
+    r.last_x = (double *)malloc(sizeof(double) * n);
+    dof = (double *)malloc(sizeof(double) * n);
+    gtmp = (double *)malloc(sizeof(double) * n);
+    memcpy(r.xc, x, sizeof(double) * 3 * N);
+    cart_to_frac(N, r.xc, r.L, r.xf);
+    str_buf(&r, dof);
+    if (mb_bfgs_init(&b, n, dof, 0.01, 0.1, relax_f, relax_fg, &r)) { rc = fail(MB_ERR_ARG, "out of memory"); goto done; }
+    if (r.err) { rc = r.err; mb_bfgs_free(&b); goto done; }
+    conv = r.maxf < fmax && r.maxu < fmax;
+    while (!conv && iter < mitr) {
+        iter++;
+        st = mb_bfgs_iterate(&b);
+        if (r.err) { rc = r.err; break; }
+        if (st != MB_BFGS_OK) break;
+        if (memcmp(r.last_x, b.x, sizeof(double) * n) != 0) {
+            /* accepted point is not the last evaluated one: refresh the criterion there */
+            memcpy(dof, b.x, sizeof(double) * n);
+            relax_fg(&r, dof, gtmp);
+            if (r.err) { rc = r.err; break; }
+        }
+        conv = r.maxf < fmax && r.maxu < fmax;
+    }
+    if (!rc) {
+        buf_str(&r, b.x);
+        frac_to_cart(N, r.xf, r.L, x);
+        memcpy(lat9, r.L, sizeof(double) * 9);
+        if (H) *H = b.f;
+        if (counts) { counts[0] = r.ne; counts[1] = r.nf; counts[2] = iter; }
+        if (converged) *converged = conv;
+    }
+    mb_bfgs_free(&b);
+done:
+    free(r.xf); free(r.xc); free(r.F); free(r.last_x); free(dof); free(gtmp);
+    return rc;
+}
 
 int mb_relax(mb_potential *p, int N, int NM, int ND, const int *atmn, double *lat9, double *x, double p_gpa,
              double urep, int rlxt, int mitr, double etol, double *H, long *counts) {

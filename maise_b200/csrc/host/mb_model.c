@@ -284,6 +284,7 @@ static int parse_basis(const mb_lines *L, mb_model *m, char *err, size_t el) {
             P->zm1bits[i] = (int)z - 1;
         }
         for (i = 0; i < P->nlam; i++) P->lam[i] = blk[0].gp[6][i];
+        P->zeta_std = P->nz == 4 && P->zeta[0] == 1.0 && P->zeta[1] == 2.0 && P->zeta[2] == 4.0 && P->zeta[3] == 16.0;
         for (f = 0; f < P->ng4; f++) {
             const int *r = gf[g4first + f];
             if (r[4] >= P->ne || r[6] >= P->nz || r[7] >= P->nlam) {

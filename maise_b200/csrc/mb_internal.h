@@ -39,6 +39,7 @@ typedef struct {
     /* angular parameters (species-0 block) */
     double zeta[MB_MAXZ], lam[MB_MAXL], powz[MB_MAXZ];
     int zeta_int;            /* all zeta are integers in [1,64]: powers by squaring */
+    int zeta_std;            /* zeta = {1, 2, 4, 16} exactly (the reference bases) */
     int zbits[MB_MAXZ];      /* bit pattern of zeta   (integer case) */
     int zm1bits[MB_MAXZ];    /* bit pattern of zeta-1 (integer case) */
     /* G4 feature f -> (eta index, zeta*nlam+lambda index) */

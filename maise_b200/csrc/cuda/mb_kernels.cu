@@ -962,6 +962,7 @@ struct EfsShape {
     int wpa, apb;
 };
 static const EfsShape kShapes[] = {{1, 4}, {4, 1}, {8, 1}};
+#define EFS_STATIC_SMEM (sizeof(mb_params) + 16) /* k_efs's __shared__ Ps, with alignment slack */
 #define MB_NSHAPES 3
 
 /* specialised kernel for the reference bases: 7 G4 exponents, 4 zeta, 2 lambda */
@@ -1025,8 +1026,10 @@ static int launch_shape(const EfsArgs &a, cudaStream_t st, cudaEvent_t e0, cudaE
     auto kern = k_efs<NE, NZ, NLAM, WPA, APB>;
     size_t smem = a.smem_group * APB;
     static size_t configured = 0;
-    if (smem > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
-    if (smem > 48 * 1024 && smem > configured) {
+    /* the 48 KB default and the 227 KB opt-in limit both count the kernel's
+     * static shared block (the staged mb_params) as well as the dynamic part */
+    if (smem + EFS_STATIC_SMEM > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
+    if (smem + EFS_STATIC_SMEM > 48 * 1024 && smem > configured) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
         configured = smem;
@@ -1073,7 +1076,7 @@ static int tune_shape(mb_dev *d, const mb_model *m, int N, int mode, const EfsAr
     int best = 0;
     float best_ms = 1e30f;
     for (int sh = 0; sh < MB_NSHAPES; sh++) {
-        if (group_bytes(m, a.cap, kShapes[sh].wpa) * kShapes[sh].apb > 227 * 1024) continue;
+        if (group_bytes(m, a.cap, kShapes[sh].wpa) * kShapes[sh].apb + EFS_STATIC_SMEM > 227 * 1024) continue;
         float ms = 1e30f;
         for (int rep = 0; rep < 2; rep++) {
             if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);

@@ -220,6 +220,27 @@ def test_capacity_growth_between_calls(mb, tmp_path):
     np.testing.assert_allclose(r["F"], ro["F"], atol=F_ATOL)
 
 
+@pytest.mark.parametrize("shape", [0, 1, 2])
+def test_every_kernel_shape_matches_oracle_at_large_capacity(mb, tmp_path, monkeypatch, shape):
+    """Each warps-per-atom shape forced in turn (the autotuner would skip a
+    shape whose launch fails), with the neighbour capacity reserved at 128
+    so that the wide shapes need more than the 48 KB default of shared
+    memory."""
+    from maise_b200 import workloads
+
+    w = workloads.random_alloy(n=3, a=3.8, seed=8, jitter=0.08)
+    d = _model_for(tmp_path, w)
+    monkeypatch.setenv("MAISE_B200_SHAPE", str(shape))
+    pot, o = mb.Potential(d + "/model"), Oracle(d + "/model")
+    pot.reserve(len(w["atmn"]), 128)
+    r = pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=200)
+    ro = o.efs(w["X"], w["LAT"], w["atmn"], 3, NM=200)
+    assert r["H"] == pytest.approx(ro["H"], rel=E_RTOL)
+    np.testing.assert_allclose(r["F"], ro["F"], atol=F_ATOL)
+    np.testing.assert_allclose(r["U"], ro["U"], rtol=E_RTOL, atol=1e-8)
+    pot.close()
+
+
 def test_nonfinite_positions_are_rejected(mb, tmp_path):
     c = load_golden("ref_efs.npz")["cases"][0]
     d = write_model_dir(tmp_path, c["model"])

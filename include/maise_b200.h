@@ -140,6 +140,32 @@ int mb_maxwell(int N, const double *amu, double T, long seed, double *v);
 /* Atomic mass (amu) of element z as tabulated by the reference (src/util.c:11). */
 double mb_atomic_mass(int z);
 
+/* Energy, forces and virial of one structure, like mb_efs, for callers that
+ * cannot let the library allocate device memory: host codes that carve every
+ * device buffer out of their own pre-sized pool or fixed memory budget, for
+ * which a cudaMalloc inside their time-step loop could exceed the budget and
+ * would synchronise the device under their streams.  This entry point has no
+ * counterpart in the reference.  It allocates nothing: inputs and outputs are
+ * the caller's device buffers, and all intermediates live in one fixed
+ * device array of about 7.3 MB that every GPU loading the library holds
+ * until the process exits.
+ *   d_x[3N]   positions (Cartesian, device); read, not modified
+ *   d_spc[N]  species (device)
+ *   lat9      lattice (host)
+ *   d_frc[3N] forces (device, written)
+ *   d_out[8]  E, H, U[6] (device, written)
+ * Limits: N <= 2048 atoms and at most 96 neighbours per atom; larger inputs
+ * are rejected with MB_ERR_CAPACITY.  The work is queued on `stream` (a
+ * cudaStream_t, 0 for the default stream) and the call returns once the
+ * stream has run it (it reads back a 16-byte status word).  The first call
+ * on a device looks up the array's device address with
+ * cudaGetSymbolAddress; make that first call before any stream capture.
+ * All calls share the one array and it keeps the last call's contents:
+ * calls that overlap on the GPU (other streams, other host threads) race
+ * and must not be issued. */
+int mb_efs_noalloc(mb_potential *pot, int N, int NM, int ND, const double *lat9, const double *d_x, const int *d_spc,
+                   double p_gpa, double urep, double *d_frc, double *d_out, void *stream);
+
 /* ---- diagnostics (no counterpart in the reference) ---- */
 
 /* Start (enable=1) or stop timing of the fused descriptor/force kernel: every

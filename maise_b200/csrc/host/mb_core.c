@@ -384,6 +384,14 @@ static void setup_cell(const mb_potential *p, const double *lat9, int ND, int N,
     }
 }
 
+/* accessors used by mb_static.cu */
+void mb_handle_geometry(const mb_potential *p, const double *lat9, int ND, int N, double p_gpa, mb_cell *c, double *pV) {
+    setup_cell(p, lat9, ND, N, c);
+    *pV = ND == 3 ? p_gpa / MB_EV2GPA * cell_volume(lat9) : 0.0;
+}
+mb_params *mb_handle_dev_params(mb_potential *p) { return p->d.params; }
+double *mb_handle_dev_weights(mb_potential *p) { return p->d.weights; }
+
 /* fractional -> Cartesian as CAST_CELL does (src/cmod.c:1108-1117) */
 static void frac_to_cart(int N, const double *xf, const double *L, double *x) {
     int i, q, j;

@@ -168,6 +168,13 @@ int mb_efs_noalloc(mb_potential *pot, int N, int NM, int ND, const double *lat9,
 
 /* ---- diagnostics (no counterpart in the reference) ---- */
 
+/* Run the NVT loop of mb_md_nvt as CUDA graphs (enable=1, the default; the
+ * environment variable MAISE_B200_GRAPHS=0 makes 0 the default) or as plain
+ * launches (0).  Each chunk of 10 steps is captured once and replayed while
+ * the buffers, sizes and step parameters it was captured for hold; results
+ * are the same either way. */
+int mb_graphs(mb_potential *p, int enable);
+
 /* Start (enable=1) or stop timing of the fused descriptor/force kernel: every
  * launch is bracketed by CUDA events on the handle's stream (up to
  * `capacity` launches), and the kernel's pair/triplet counters are reset. */

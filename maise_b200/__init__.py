@@ -67,6 +67,7 @@ def load_library():
     lib.mb_stream.argtypes = [vp]
     lib.mb_launch_count.restype = ctypes.c_long
     lib.mb_launch_count.argtypes = [vp]
+    lib.mb_graphs.argtypes = [vp, c_i]
     lib.mb_profile.argtypes = [vp, c_i, c_i]
     lib.mb_profile_read.argtypes = [vp, _D, _I, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
     lib.mb_fp64_peak.argtypes = [c_i, _D]
@@ -185,6 +186,10 @@ class Potential:
         ms, n = ctypes.c_double(), ctypes.c_int()
         self._check(self.lib.mb_md_profile_read(self.h, ctypes.byref(ms), ctypes.byref(n)))
         return dict(ms_total=ms.value, steps=n.value)
+
+    def graphs(self, enable: bool) -> None:
+        """MD chunks as CUDA graphs (default) or plain launches."""
+        self._check(self.lib.mb_graphs(self.h, 1 if enable else 0))
 
     def reserve(self, max_atoms: int, max_neighbours: int) -> None:
         self._check(self.lib.mb_reserve(self.h, max_atoms, max_neighbours))

@@ -906,9 +906,11 @@ __global__ void k_finalize(int N, int mode, double pV, const double *EA, const d
 /* ------------------------------------------------------------------ */
 
 /* K = 1/2 sum m v^2 in atom order, then xi += dt/tau^2 (2K/(3NT) - 1).
- * out[8] = K, out[9] = xi; trace[2*step] = H, trace[2*step+1] = K. */
+ * out[8] = K, out[9] = xi; trace[2*step] = H, trace[2*step+1] = K with the
+ * step index kept in out[10] and advanced here, so that a captured chunk of
+ * steps can be replayed unchanged. */
 __global__ void k_nvt_thermostat(int N, const double *V, const int *spc, const double *mass, double dt, double tau,
-                                 double T, int step, double *out, double *trace, int capTrace) {
+                                 double T, double *out, double *trace, int capTrace) {
     __shared__ double red[256];
     int t = threadIdx.x;
     double k = 0.0;
@@ -925,8 +927,10 @@ __global__ void k_nvt_thermostat(int N, const double *V, const int *spc, const d
     if (t == 0) {
         double K = 0.5 * red[0];
         double fs = 1.0 / (tau * tau) * (2.0 * K / ((3.0 * (double)N) * T) - 1.0);
+        const int step = (int)out[10];
         out[8] = K;
         out[9] += dt * fs;
+        out[10] = (double)(step + 1);
         if (step >= 0 && step < capTrace) {
             trace[2 * step] = out[1];
             trace[2 * step + 1] = K;
@@ -1034,9 +1038,9 @@ static int launch_shape(const EfsArgs &a, cudaStream_t st, cudaEvent_t e0, cudaE
         if (e != cudaSuccess) return (int)e;
         configured = smem;
     }
-    if (e0) cudaEventRecord(e0, st);
+    if (e0) mbk_record(e0, st);
     kern<<<(a.N + APB - 1) / APB, WPA * 32 * APB, smem, st>>>(a);
-    if (e1) cudaEventRecord(e1, st);
+    if (e1) mbk_record(e1, st);
     return (int)cudaGetLastError();
 }
 
@@ -1143,19 +1147,42 @@ extern "C" int mbk_finalize(mb_dev *d, int N, int mode, double pV, void *stream,
     return (int)cudaGetLastError();
 }
 
-extern "C" int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, int step,
-                              void *stream, long *launches) {
+extern "C" int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, void *stream,
+                              long *launches) {
     cudaStream_t st = (cudaStream_t)stream;
     (void)m;
     /* masses by species live after the weights in the parameter upload (see mb_core.c) */
     const double *mass = d->weights + m->weights_len;
-    k_nvt_thermostat<<<1, 256, 0, st>>>(N, d->V, d->spc, mass, dt, tau, T, step, d->out, d->trace, d->capTrace);
+    k_nvt_thermostat<<<1, 256, 0, st>>>(N, d->V, d->spc, mass, dt, tau, T, d->out, d->trace, d->capTrace);
     k_nvt_integrate<<<(N + 127) / 128, 128, 0, st>>>(N, d->X, d->V, d->F, d->spc, mass, dt, d->out);
     *launches += 2;
     return (int)cudaGetLastError();
 }
 
-extern "C" int mbk_set_xi(mb_dev *d, double xi, void *stream) {
-    k_set_out<<<1, 1, 0, (cudaStream_t)stream>>>(d->out, 9, xi);
+extern "C" int mbk_set_out(mb_dev *d, int idx, double v, void *stream) {
+    k_set_out<<<1, 1, 0, (cudaStream_t)stream>>>(d->out, idx, v);
     return (int)cudaGetLastError();
+}
+
+/* events recorded while the stream is being captured become event-record
+ * nodes of the graph, so that they time every replay */
+extern "C" void mbk_record(void *event, void *stream) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing((cudaStream_t)stream, &cs);
+    if (cs == cudaStreamCaptureStatusActive)
+        cudaEventRecordWithFlags((cudaEvent_t)event, (cudaStream_t)stream, cudaEventRecordExternal);
+    else
+        cudaEventRecord((cudaEvent_t)event, (cudaStream_t)stream);
+}
+
+/* 1 when the descriptor pass of (N, mode) at the current capacity has its
+ * kernel shape already: only then may it be captured (tuning synchronises) */
+extern "C" int mbk_shape_ready(const mb_dev *d, int N, int mode) {
+    int bucket = 0, k;
+    if (d->tune_fixed >= 0) return 1;
+    while ((1 << bucket) < N) bucket++;
+    const int key = (mode << 28) | (bucket << 20) | (d->capNB & 0xfffff);
+    for (k = 0; k < d->tune_n; k++)
+        if (d->tune_key[k] == key) return 1;
+    return 0;
 }

@@ -22,6 +22,17 @@
 #define MB_KB_INV 11604.0           /* K per eV, src/cmod.c:5 */
 #define MB_PI 3.1415926535897932384626433832795
 
+/* what an MD chunk graph was captured for: it is replayed only while all
+ * of this is unchanged (buffers, sizes, step parameters, profiling state) */
+typedef struct {
+    long gen;
+    int N, NM, chunk, st_on, ev_on;
+    double urep, dt, tau, T;
+    mb_cell c;
+    void *flush, *trace, *st_pool, *ev_pool;
+    size_t flush_bytes;
+} md_key;
+
 struct mb_potential {
     mb_model m;
     int device;
@@ -30,11 +41,21 @@ struct mb_potential {
     cudaStream_t stream;
     mb_dev d;
     long launches;
+    long gen; /* advanced whenever device buffers are reallocated */
     /* host staging (pinned) */
     double *h_buf;
     size_t h_buf_len;
     int *h_status;
     double *h_out;
+    /* MD chunk graph */
+    int use_graphs;
+    cudaGraphExec_t md_exec;
+    md_key md_k;
+    long md_launches;
+    int md_st_events, md_ev_events;
+    /* timings moved out of the event pools (graph replays reuse the events) */
+    double st_acc_ms, ev_acc_ms;
+    int st_acc_n, ev_acc_n;
 };
 
 static __thread char mb_err[512];
@@ -83,6 +104,10 @@ int mb_open(const char *model_path, int device, mb_potential **out) {
     p->device = device;
     p->d.tune_fixed = -1;
     {
+        const char *g = getenv("MAISE_B200_GRAPHS");
+        p->use_graphs = !(g && g[0] == '0');
+    }
+    {
         const char *fx = getenv("MAISE_B200_SHAPE");
         if (fx) p->d.tune_fixed = atoi(fx);
     }
@@ -119,6 +144,7 @@ int mb_close(mb_potential *p) {
     if (!p) return MB_OK;
     cudaSetDevice(p->device);
     cudaStreamSynchronize(p->stream);
+    if (p->md_exec) cudaGraphExecDestroy(p->md_exec);
     dev_free(&p->d);
     cudaFree(p->d.params);
     cudaFree(p->d.weights);
@@ -195,6 +221,8 @@ int mb_profile(mb_potential *p, int enable, int capacity) {
     }
     d->ev_on = enable ? 1 : 0;
     d->ev_n = 0;
+    p->ev_acc_ms = 0.0;
+    p->ev_acc_n = 0;
     CK(cudaMemsetAsync(d->counters, 0, sizeof(unsigned long long) * 2, p->stream), "memset counters");
     CK(cudaStreamSynchronize(p->stream), "synchronize");
     return MB_OK;
@@ -226,6 +254,8 @@ int mb_md_profile(mb_potential *p, int enable, int capacity, size_t flush_bytes)
     if (enable) d->flush_bytes = flush_bytes > d->flush_bytes ? flush_bytes : d->flush_bytes;
     d->st_on = enable ? 1 : 0;
     d->st_n = 0;
+    p->st_acc_ms = 0.0;
+    p->st_acc_n = 0;
     return MB_OK;
 }
 
@@ -241,8 +271,8 @@ int mb_md_profile_read(mb_potential *p, double *total_ms, int *steps) {
            "cudaEventElapsedTime");
         tot += ms;
     }
-    if (total_ms) *total_ms = tot;
-    if (steps) *steps = p->d.st_n;
+    if (total_ms) *total_ms = tot + p->st_acc_ms;
+    if (steps) *steps = p->d.st_n + p->st_acc_n;
     return MB_OK;
 }
 
@@ -261,13 +291,19 @@ int mb_profile_read(mb_potential *p, double *total_ms, int *launches, unsigned l
         tot += ms;
     }
     CK(cudaMemcpy(c, p->d.counters, sizeof(c), cudaMemcpyDeviceToHost), "D2H counters");
-    if (total_ms) *total_ms = tot;
-    if (launches) *launches = p->d.ev_n;
+    if (total_ms) *total_ms = tot + p->ev_acc_ms;
+    if (launches) *launches = p->d.ev_n + p->ev_acc_n;
     if (pairs) *pairs = c[0];
     if (triplets) *triplets = c[1];
     return MB_OK;
 }
 long mb_launch_count(const mb_potential *p) { return p ? p->launches : 0; }
+
+int mb_graphs(mb_potential *p, int enable) {
+    if (!p) return fail(MB_ERR_ARG, "null handle");
+    p->use_graphs = enable ? 1 : 0;
+    return MB_OK;
+}
 
 /* grow device arrays to N atoms / nb neighbours per atom / ncell bins */
 static int ensure(mb_potential *p, int N, int nb, int ncell) {
@@ -289,6 +325,7 @@ static int ensure(mb_potential *p, int N, int nb, int ncell) {
         CK(cudaMalloc((void **)&d->cell_of, sizeof(int) * cap), "alloc cell_of");
         CK(cudaMalloc((void **)&d->cell_atoms, sizeof(int) * cap), "alloc cell_atoms");
         d->capN = cap;
+        p->gen++;
         cudaFree(d->nj); cudaFree(d->nd);
         d->nj = NULL; d->nd = NULL;
         d->capNB = 0;
@@ -300,6 +337,7 @@ static int ensure(mb_potential *p, int N, int nb, int ncell) {
         CK(cudaMalloc((void **)&d->nj, sizeof(int) * (size_t)cap * d->capN), "alloc nj");
         CK(cudaMalloc((void **)&d->nd, sizeof(double) * 4 * (size_t)cap * d->capN), "alloc nd");
         d->capNB = cap;
+        p->gen++;
     }
     if (ncell + 1 > d->capCells) {
         int cap = ncell + 1 > 2 * d->capCells ? ncell + 1 : 2 * d->capCells;
@@ -307,6 +345,7 @@ static int ensure(mb_potential *p, int N, int nb, int ncell) {
         CK(cudaMalloc((void **)&d->cell_cnt, sizeof(int) * cap), "alloc cell_cnt");
         CK(cudaMalloc((void **)&d->cell_start, sizeof(int) * (cap + 1)), "alloc cell_start");
         d->capCells = cap;
+        p->gen++;
     }
     return MB_OK;
 }
@@ -767,6 +806,130 @@ done:
 /* NVT molecular dynamics                                              */
 /* ------------------------------------------------------------------ */
 
+/* Move the times of the recorded step and kernel events into the
+ * accumulators and free the pool slots (the stream must be idle). */
+static int harvest_events(mb_potential *p) {
+    int k;
+    for (k = 0; k < p->d.st_n; k++) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, ((cudaEvent_t *)p->d.st_pool)[2 * k], ((cudaEvent_t *)p->d.st_pool)[2 * k + 1]),
+           "cudaEventElapsedTime");
+        p->st_acc_ms += ms;
+        p->st_acc_n++;
+    }
+    for (k = 0; k < p->d.ev_n; k++) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, ((cudaEvent_t *)p->d.ev_pool)[2 * k], ((cudaEvent_t *)p->d.ev_pool)[2 * k + 1]),
+           "cudaEventElapsedTime");
+        p->ev_acc_ms += ms;
+        p->ev_acc_n++;
+    }
+    p->d.st_n = 0;
+    p->d.ev_n = 0;
+    return MB_OK;
+}
+
+/* One MD step of Dynamics' NVT branch: CELL_FRC (wrap + list + descriptor
+ * pass + finalize), thermostat and integrator, then JAR.  With step
+ * profiling on, the L2 is overwritten before the step, outside its events. */
+static int md_step(mb_potential *p, int N, int NM, const mb_cell *c, double urep, double dt, double tau, double T,
+                   int tag) {
+    cudaEvent_t t1 = 0;
+    int r;
+    if (p->d.st_on && p->d.flush)
+        CK(cudaMemsetAsync(p->d.flush, tag & 0xff, p->d.flush_bytes, p->stream), "flush");
+    if (p->d.st_on && p->d.st_n < p->d.st_cap) {
+        mbk_record(((cudaEvent_t *)p->d.st_pool)[2 * p->d.st_n], p->stream);
+        t1 = ((cudaEvent_t *)p->d.st_pool)[2 * p->d.st_n + 1];
+        p->d.st_n++;
+    }
+    if ((r = mbk_wrap(&p->d, N, c, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "wrap");
+    if ((r = mbk_nlist(&p->d, N, NM, c, p->m.rc_list, p->stream, &p->launches)))
+        return cuda_fail((cudaError_t)r, "neighbour list");
+    if ((r = mbk_descriptor_pass(&p->d, &p->m, N, MB_MODE_EFS, urep, 0, 0, p->stream, &p->launches)))
+        return cuda_fail((cudaError_t)r, "descriptor kernel");
+    if ((r = mbk_finalize(&p->d, N, MB_MODE_EFS, 0.0, p->stream, &p->launches)))
+        return cuda_fail((cudaError_t)r, "finalize");
+    if ((r = mbk_nvt_update(&p->d, &p->m, N, dt, tau, T / MB_KB_INV, p->stream, &p->launches)))
+        return cuda_fail((cudaError_t)r, "integrator");
+    if ((r = mbk_wrap(&p->d, N, c, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "wrap");
+    if (t1) mbk_record(t1, p->stream);
+    return MB_OK;
+}
+
+/* Queue `chunk` MD steps from `step` on.  They run as one CUDA graph,
+ * captured on first use and replayed while nothing it was captured for has
+ * changed; a chunk whose kernel shape is not tuned yet (tuning times launches
+ * and synchronises) runs as plain launches.  *graphed tells which. */
+static int md_chunk(mb_potential *p, int N, int NM, const mb_cell *c, double urep, double dt, double tau, double T,
+                    int step, int chunk, int *graphed) {
+    int r, s;
+    *graphed = 0;
+    CK(cudaMemsetAsync(p->d.status, 0, sizeof(int) * 4, p->stream), "memset status");
+    if ((r = mbk_set_out(&p->d, 10, (double)step, p->stream))) return cuda_fail((cudaError_t)r, "set step");
+    if (p->use_graphs && mbk_shape_ready(&p->d, N, MB_MODE_EFS)) {
+        md_key k;
+        memset(&k, 0, sizeof(k));
+        k.gen = p->gen;
+        k.N = N;
+        k.NM = NM;
+        k.chunk = chunk;
+        k.st_on = p->d.st_on;
+        k.ev_on = p->d.ev_on;
+        k.urep = urep;
+        k.dt = dt;
+        k.tau = tau;
+        k.T = T;
+        k.c = *c;
+        k.flush = p->d.flush;
+        k.flush_bytes = p->d.flush_bytes;
+        k.trace = p->d.trace;
+        k.st_pool = p->d.st_pool;
+        k.ev_pool = p->d.ev_pool;
+        if (!p->md_exec || memcmp(&k, &p->md_k, sizeof(k))) {
+            cudaGraph_t g = NULL;
+            cudaError_t e;
+            const long l0 = p->launches;
+            if (p->md_exec) {
+                cudaGraphExecDestroy(p->md_exec);
+                p->md_exec = NULL;
+            }
+            /* the captured events take the first pool slots */
+            CK(cudaStreamSynchronize(p->stream), "synchronize");
+            if ((r = harvest_events(p))) return r;
+            CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            for (s = 0; s < chunk; s++)
+                if ((r = md_step(p, N, NM, c, urep, dt, tau, T, s))) break;
+            e = cudaStreamEndCapture(p->stream, &g);
+            if (r) {
+                if (g) cudaGraphDestroy(g);
+                return r;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "end capture");
+            e = cudaGraphInstantiate(&p->md_exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                p->md_exec = NULL;
+                return cuda_fail(e, "graph instantiate");
+            }
+            p->md_k = k;
+            p->md_launches = p->launches - l0;
+            p->launches = l0;
+            p->md_st_events = p->d.st_n;
+            p->md_ev_events = p->d.ev_n;
+            p->d.st_n = 0;
+            p->d.ev_n = 0;
+        }
+        CK(cudaGraphLaunch(p->md_exec, p->stream), "graph launch");
+        p->launches += p->md_launches;
+        *graphed = 1;
+        return MB_OK;
+    }
+    for (s = 0; s < chunk; s++)
+        if ((r = md_step(p, N, NM, c, urep, dt, tau, T, step + s))) return r;
+    return MB_OK;
+}
+
 int mb_md_nvt(mb_potential *p, int N, int NM, int ND, const int *atmn, const double *lat9, double *x, double *v,
               double T, double dt, double tau, int nsteps, double urep, double *xi, double *Hs, double *Ks) {
     mb_cell c;
@@ -792,12 +955,12 @@ int mb_md_nvt(mb_potential *p, int N, int NM, int ND, const int *atmn, const dou
         r = run_pass(p, N, NM, ND, lat9, MB_MODE_EFS, urep, 0.0);
     }
     if (r) return r == MB_RETRY ? fail(MB_ERR_CAPACITY, "neighbour capacity could not be established") : r;
-    if ((r = mbk_set_xi(&p->d, xi0, p->stream))) return cuda_fail((cudaError_t)r, "set xi");
+    if ((r = mbk_set_out(&p->d, 9, xi0, p->stream))) return cuda_fail((cudaError_t)r, "set xi");
     /* checkpoints for re-running a chunk whose neighbour counts outgrew the capacity */
     CK(cudaMalloc((void **)&X0, sizeof(double) * 3 * N), "alloc checkpoint");
     CK(cudaMalloc((void **)&V0, sizeof(double) * 3 * N), "alloc checkpoint");
     for (step = 0; step < nsteps; step += chunk) {
-        int s, attempt;
+        int attempt, graphed = 0;
         double xis;
         chunk = nsteps - step < 10 ? nsteps - step : 10;
         CK(cudaMemcpyAsync(X0, p->d.X, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, p->stream), "checkpoint");
@@ -806,31 +969,8 @@ int mb_md_nvt(mb_potential *p, int N, int NM, int ND, const int *atmn, const dou
         CK(cudaStreamSynchronize(p->stream), "synchronize");
         xis = p->h_out[9];
         for (attempt = 0; attempt < 3; attempt++) {
-            CK(cudaMemsetAsync(p->d.status, 0, sizeof(int) * 4, p->stream), "memset status");
-            for (s = 0; s < chunk; s++) {
-                cudaEvent_t t1 = 0;
-                if (p->d.st_on && p->d.flush) {
-                    /* overwrite L2 between steps, outside the timed region */
-                    CK(cudaMemsetAsync(p->d.flush, (step + s) & 0xff, p->d.flush_bytes, p->stream), "flush");
-                }
-                if (p->d.st_on && p->d.st_n < p->d.st_cap) {
-                    CK(cudaEventRecord(((cudaEvent_t *)p->d.st_pool)[2 * p->d.st_n], p->stream), "event");
-                    t1 = ((cudaEvent_t *)p->d.st_pool)[2 * p->d.st_n + 1];
-                    p->d.st_n++;
-                }
-                /* CELL_FRC (wrap + list + descriptor pass), then thermostat and integrator, then JAR */
-                if ((r = mbk_wrap(&p->d, N, &c, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "wrap");
-                if ((r = mbk_nlist(&p->d, N, NM, &c, p->m.rc_list, p->stream, &p->launches)))
-                    return cuda_fail((cudaError_t)r, "neighbour list");
-                if ((r = mbk_descriptor_pass(&p->d, &p->m, N, MB_MODE_EFS, urep, 0, 0, p->stream, &p->launches)))
-                    return cuda_fail((cudaError_t)r, "descriptor kernel");
-                if ((r = mbk_finalize(&p->d, N, MB_MODE_EFS, 0.0, p->stream, &p->launches)))
-                    return cuda_fail((cudaError_t)r, "finalize");
-                if ((r = mbk_nvt_update(&p->d, &p->m, N, dt, tau, T / MB_KB_INV, step + s, p->stream, &p->launches)))
-                    return cuda_fail((cudaError_t)r, "integrator");
-                if ((r = mbk_wrap(&p->d, N, &c, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "wrap");
-                if (t1) CK(cudaEventRecord(t1, p->stream), "event");
-            }
+            const int st0 = p->d.st_n, ev0 = p->d.ev_n;
+            if ((r = md_chunk(p, N, NM, &c, urep, dt, tau, T, step, chunk, &graphed))) goto out;
             CK(cudaMemcpyAsync(p->h_status, p->d.status, sizeof(int) * 4, cudaMemcpyDeviceToHost, p->stream), "D2H status");
             CK(cudaStreamSynchronize(p->stream), "synchronize");
             if (p->h_status[0] & MB_ST_WRAP) { r = fail(MB_ERR_STATE, "non-finite positions in MD"); goto out; }
@@ -838,13 +978,22 @@ int mb_md_nvt(mb_potential *p, int N, int NM, int ND, const int *atmn, const dou
                 r = fail(MB_ERR_NEIGHBOURS, "an atom reached NM=%d neighbours during MD", NM);
                 goto out;
             }
-            if (!(p->h_status[0] & MB_ST_CAP_OVERFLOW)) break;
-            /* grow and replay the chunk from its checkpoint (its step timings are dropped) */
-            if (p->d.st_on) p->d.st_n = p->d.st_n >= chunk ? p->d.st_n - chunk : 0;
+            if (!(p->h_status[0] & MB_ST_CAP_OVERFLOW)) {
+                if (graphed) {
+                    /* the replay re-recorded the graph's events: move their times out */
+                    p->d.st_n = p->md_st_events;
+                    p->d.ev_n = p->md_ev_events;
+                    if ((r = harvest_events(p))) goto out;
+                }
+                break;
+            }
+            /* grow and replay the chunk from its checkpoint (its timings are dropped) */
+            p->d.st_n = graphed ? 0 : st0;
+            p->d.ev_n = graphed ? 0 : ev0;
             if ((r = ensure(p, N, p->h_status[1] + 8, c.M[0] ? c.M[0] * c.M[1] * c.M[2] : 1))) goto out;
             CK(cudaMemcpyAsync(p->d.X, X0, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, p->stream), "restore");
             CK(cudaMemcpyAsync(p->d.V, V0, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, p->stream), "restore");
-            if ((r = mbk_set_xi(&p->d, xis, p->stream))) { r = cuda_fail((cudaError_t)r, "set xi"); goto out; }
+            if ((r = mbk_set_out(&p->d, 9, xis, p->stream))) { r = cuda_fail((cudaError_t)r, "set xi"); goto out; }
         }
         if (attempt == 3) { r = fail(MB_ERR_CAPACITY, "neighbour capacity could not be established"); goto out; }
     }

@@ -139,9 +139,11 @@ int mbk_nlist(mb_dev *d, int N, int NM, const mb_cell *c, double rc, void *strea
 int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode, double urep, int need_nb_max, int nb_max,
                         void *stream, long *launches);
 int mbk_finalize(mb_dev *d, int N, int mode, double pV, void *stream, long *launches);
-int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, int step, void *stream,
+int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, void *stream,
                    long *launches);
-int mbk_set_xi(mb_dev *d, double xi, void *stream);
+int mbk_set_out(mb_dev *d, int idx, double v, void *stream);
+void mbk_record(void *event, void *stream);
+int mbk_shape_ready(const mb_dev *d, int N, int mode);
 size_t mbk_efs_smem(const mb_model *m, int capNB, int shape);
 
 #ifdef __cplusplus

@@ -118,3 +118,33 @@ def test_md_results_independent_of_chunking(mb, tmp_path):
     b2 = pot.md_nvt(b1["X"], w["LAT"], w["atmn"], b1["V"], 900.0, nsteps=8, NM=200, xi=b1["xi"])
     np.testing.assert_allclose(b2["X"], a["X"], atol=1e-12)
     np.testing.assert_allclose(b2["H"], a["H"][7:], rtol=1e-13)
+
+
+@pytest.mark.parametrize("size", [2, 5])
+def test_md_graph_replay_equals_plain_launches(mb, tmp_path, size):
+    """The NVT loop replayed as captured CUDA graphs (chunks of 10 steps, a
+    shorter last chunk, a second call reusing the graph) gives the trajectory
+    of plain launches; 32 atoms take the all-pairs list, 500 the cell list."""
+    from maise_b200 import atomic_mass, maxwell, models, workloads
+
+    w = workloads.random_alloy(n=size, a=3.8, seed=9, species=(29, 46), jitter=0.05)
+    d = tmp_path / "m"
+    d.mkdir()
+    models.random_model(str(d / "model"), w["spcz"], models.Basis(), (w["X"], w["LAT"], w["atmn"], 3), seed=2)
+    N = len(w["atmn"])
+    V = maxwell([atomic_mass(w["spcz"][s]) for s in w["atmn"]], 600.0, seed=3)
+    runs = []
+    for graphs in (False, True):
+        pot = mb.Potential(str(d / "model"))
+        pot.graphs(graphs)
+        a = pot.md_nvt(w["X"], w["LAT"], w["atmn"], V, 600.0, nsteps=23, NM=200)
+        b = pot.md_nvt(a["X"], w["LAT"], w["atmn"], a["V"], 600.0, nsteps=20, NM=200, xi=a["xi"])
+        runs.append((a, b, pot.launches))
+        pot.close()
+    (a0, b0, n0), (a1, b1, n1) = runs
+    for r0, r1 in ((a0, a1), (b0, b1)):
+        np.testing.assert_allclose(r1["X"], r0["X"], atol=1e-9)
+        np.testing.assert_allclose(r1["V"], r0["V"], atol=1e-9)
+        np.testing.assert_allclose(r1["H"], r0["H"], rtol=1e-11, atol=1e-9 * N)
+        assert r1["xi"] == pytest.approx(r0["xi"], rel=1e-9, abs=1e-12)
+    assert n1 == n0  # the replays count the launches they contain

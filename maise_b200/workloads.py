@@ -68,8 +68,10 @@ def _min_image_dist(L, xf_new, xf_old):
     return best
 
 
-def random_cell(N, rng, species_count, vol_per_atom=20.0, spread=0.15, dmin=2.0, max_tries=200):
-    """EA-style random structure (cf. RAND_CL, src/eutl.c:276-390)."""
+def random_cell(N, rng, species_count, vol_per_atom=20.0, spread=0.15, dmin=2.0, max_tries=200, composition=None):
+    """EA-style random structure (cf. RAND_CL, src/eutl.c:276-390).  Species
+    are drawn at random unless `composition` gives integer ratios (N must be
+    a multiple of their sum), as in an EA run at fixed stoichiometry."""
     for _ in range(max_tries):
         V = N * vol_per_atom * (1.0 + spread * rng.uniform(-1, 1))
         ang = rng.uniform(60.0, 120.0, 3)
@@ -94,20 +96,33 @@ def random_cell(N, rng, species_count, vol_per_atom=20.0, spread=0.15, dmin=2.0,
                 break
         if not ok:
             continue
-        comp = rng.integers(0, species_count, N)
-        if species_count > 1 and len(np.unique(comp)) < 2:
-            comp[0] = (comp[0] + 1) % species_count
+        if composition is None:
+            comp = rng.integers(0, species_count, N)
+            if species_count > 1 and len(np.unique(comp)) < 2:
+                comp[0] = (comp[0] + 1) % species_count
+        else:
+            unit = sum(composition)
+            if N % unit:
+                raise ValueError(f"{N} atoms do not fit composition {composition}")
+            comp = rng.permutation(np.repeat(np.arange(len(composition)), np.asarray(composition) * (N // unit)))
         X, atmn = _group(xf @ L, comp.astype(np.int32))
         return X, L, atmn
     raise RuntimeError("could not place atoms")
 
 
-def ea_population(count=256, nmin=8, nmax=64, seed=0, species=(12, 20)):
+def ea_population(count=256, nmin=8, nmax=64, seed=0, species=(12, 20), composition=None):
+    """`count` random cells of nmin..nmax atoms (uniform); with a fixed
+    `composition` the atom count is uniform over its multiples in range."""
     rng = np.random.default_rng(seed)
     out = []
+    unit = sum(composition) if composition is not None else 1
+    sizes = [n for n in range(nmin, nmax + 1) if n % unit == 0]
     for _ in range(count):
-        N = int(rng.integers(nmin, nmax + 1))
-        X, L, atmn = random_cell(N, rng, len(species))
+        if composition is None:
+            N = int(rng.integers(nmin, nmax + 1))
+        else:
+            N = int(sizes[rng.integers(0, len(sizes))])
+        X, L, atmn = random_cell(N, rng, len(species), composition=composition)
         out.append(dict(X=X, LAT=L, atmn=atmn, ND=3, spcz=list(species)))
     return out
 

@@ -18,7 +18,7 @@ LIB = os.path.join(ROOT, "maise_b200", "libmaise_b200.so")
 
 def _declared_functions():
     names = []
-    for h in ("maise_b200.h", "maise_call.h"):
+    for h in ("maise_b200.h", "maise_call.h", "maise_surrogate.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names += re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*?[\s\*]+\**([A-Za-z_][A-Za-z0-9_]*)\s*\(",
@@ -71,6 +71,11 @@ def test_no_gpu_path_fails_loudly(lib, tmp_path):
     (tmp_path / "model").write_text(str(g["model"]))
     with pytest.raises(MaiseError) as e:
         Potential(str(tmp_path / "model"))
+    assert e.value.code == 6
+    from maise_b200.surrogate import Surrogate
+
+    with pytest.raises(MaiseError) as e:
+        Surrogate(3)
     assert e.value.code == 6
 
 

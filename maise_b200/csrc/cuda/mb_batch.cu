@@ -34,6 +34,7 @@ constexpr int BMAXDOF = 3 * BMAXN + 9;
 constexpr int BMAXD = 288;
 constexpr int BTL = 1024;
 constexpr int BWARPS = 4;
+constexpr int BIMG = 4; /* image shifts a lane holds in the fast neighbour search (128 images) */
 constexpr int BNE = 7, BNZ = 4, BNLAM = 2, BNZL = 8, BCELLS = 64;
 
 /* FP32 copy of the descriptor parameters (fast basis layout only) */
@@ -46,6 +47,7 @@ struct BParams {
     float d_eta2[MB_MAXG2], d_rs[MB_MAXG2], d_eta4[MB_MAXE];
     float lam[MB_MAXL], powz[MB_MAXZ], zeta[MB_MAXZ];
     int zbits[MB_MAXZ], zm1bits[MB_MAXZ];
+    int zstd; /* zeta = {1, 2, 4, 16} in this order */
     int g4_cell[MB_MAXG4];
     double rm[MB_MAXSPC];
     double rc;
@@ -56,6 +58,7 @@ struct BArgs {
     int S, rlxt, mitr;
     double p_ev, urep, fmax, sigma;
     const int *nat, *off, *spc;
+    const int *order; /* queue position -> structure (largest first) */
     double *lat, *x, *H;
     int *iters, *status;
     const BParams *P;
@@ -115,6 +118,22 @@ __device__ __forceinline__ void fcutf_d(float rc, float r, float &f, float &df) 
 }
 
 __device__ __forceinline__ void angularf(const BParams &P, float c, float *lz, float *lzp) {
+    if (P.zstd) {
+        /* zeta = 1, 2, 4, 16: (1 + lam c)^zeta by squaring, and the
+         * zeta - 1 = 0, 1, 3, 15 powers of the derivative from the same squares */
+#pragma unroll
+        for (int l = 0; l < BNLAM; l++) {
+            const float lam = P.lam[l], b1 = 1.0f + lam * c, b2 = b1 * b1, b4 = b2 * b2, b8 = b4 * b4;
+            const float pw[4] = {b1, b2, b4, b8 * b8};
+            const float pm[4] = {1.0f, b1, b2 * b1, b8 * b4 * b2 * b1};
+#pragma unroll
+            for (int z = 0; z < 4; z++) {
+                lz[z * BNLAM + l] = P.powz[z] * pw[z];
+                if (lzp) lzp[z * BNLAM + l] = P.powz[z] * P.zeta[z] * lam * pm[z];
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int l = 0; l < BNLAM; l++) {
         float lam = P.lam[l], base = 1.0f + lam * c;
@@ -146,6 +165,24 @@ __device__ __forceinline__ float bsumf(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULLM, v, o);
     return v;
+}
+
+/* Sum of 64 per-lane accumulators across the warp by recursive halving: at
+ * each step a lane keeps one half of its cells and adds its partner's copy
+ * of that half (32 + 16 + 8 + 4 + 2 exchanges).  On return lane l holds the
+ * totals of cells 2l and 2l+1 in v[0], v[1]. */
+__device__ __forceinline__ void warp_reduce64f(float *v, int lane) {
+#pragma unroll
+    for (int step = 0; step < 5; step++) {
+        const int off = 16 >> step, half = 32 >> step;
+        const bool upper = (lane & off) != 0;
+#pragma unroll
+        for (int k = 0; k < half; k++) {
+            const float send = upper ? v[k] : v[k + half];
+            const float keep = upper ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(FULLM, send, off);
+        }
+    }
 }
 
 /* CTA-wide sum of one double per thread (all threads get the result) */
@@ -331,11 +368,10 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
             }
             ws.blk[blkid][0] = start;
             ws.blk[blkid][1] = tl_pos;
-            /* lane sums in FP64 across the warp */
-            for (int cell = 0; cell < BCELLS; cell++) {
-                double t = bsum((double)acc[cell]);
-                if (lane == 0) ws.red[cell] = t;
-            }
+            /* lane sums across the warp */
+            warp_reduce64f(acc, lane);
+            ws.red[2 * lane] = acc[0];
+            ws.red[2 * lane + 1] = acc[1];
             __syncwarp();
             if (lane == 0) {
                 int base = P.ind4[a * a + b * b];
@@ -405,8 +441,6 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
         float v0 = cr * d.x, v1 = cr * d.y, v2 = cr * d.z;
         fi0 += v0; fi1 += v1; fi2 += v2;
         ws.Fnb[3 * t] = -v0; ws.Fnb[3 * t + 1] = -v1; ws.Fnb[3 * t + 2] = -v2;
-        vr[0] -= (double)(v0 * d.x); vr[1] -= (double)(v1 * d.y); vr[2] -= (double)(v2 * d.z);
-        vr[3] -= (double)(v0 * d.y); vr[4] -= (double)(v1 * d.z); vr[5] -= (double)(v2 * d.x);
         if (A.urep > 0.0) {
             double R = P.rm[s0] + P.rm[ws.sp[t]], rd = (double)r;
             if (rd < R) {
@@ -452,13 +486,22 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
                     lo = 0;
                     __syncwarp();
                 }
-                for (int t = lo + lane; t < hi; t += 32) {
-                    unsigned pk = ws.tl[t];
-                    int jj = pk & 0xffff, kk = pk >> 16;
+                for (int base = lo; base < hi; base += 32) {
+                    /* lanes take consecutive list entries; the list runs row by row,
+                     * so lanes with the same j are adjacent (key -1-lane past the end) */
+                    const int t = base + lane;
+                    int jj = -1 - lane, kk = 0;
+                    bool on = false;
+                    float g1x = 0.0f, g1y = 0.0f, g1z = 0.0f, g2x = 0.0f, g2y = 0.0f, g2z = 0.0f;
+                    if (t < hi) {
+                    const unsigned pk = ws.tl[t];
+                    jj = pk & 0xffff;
+                    kk = pk >> 16;
                     float4 d1 = ws.d[jj], d2 = ws.d[kk];
                     float wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
                     float r3s = wx * wx + wy * wy + wz * wz, r3 = sqrtf(r3s);
-                    if (!(d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq)) continue;
+                    on = d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq;
+                    if (on) {
                     float r1 = d1.w, r2 = d2.w, ir1 = ws.ir[jj], ir2 = ws.ir[kk], ir3 = 1.0f / r3;
                     float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
                     float f3, df3;
@@ -488,24 +531,52 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
                     float Tc = Af * Qc;
                     float a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
                     float a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
-                    float g1x = a11 * d1.x + a12 * d2.x - a3 * wx, g1y = a11 * d1.y + a12 * d2.y - a3 * wy,
-                          g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
-                    float g2x = a22 * d2.x + a12 * d1.x + a3 * wx, g2y = a22 * d2.y + a12 * d1.y + a3 * wy,
-                          g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                    g1x = a11 * d1.x + a12 * d2.x - a3 * wx;
+                    g1y = a11 * d1.y + a12 * d2.y - a3 * wy;
+                    g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
+                    g2x = a22 * d2.x + a12 * d1.x + a3 * wx;
+                    g2y = a22 * d2.y + a12 * d1.y + a3 * wy;
+                    g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                    }
+                    }
                     fi0 += g1x + g2x; fi1 += g1y + g2y; fi2 += g1z + g2z;
-                    atomicAdd(&ws.Fnb[3 * jj], -g1x); atomicAdd(&ws.Fnb[3 * jj + 1], -g1y); atomicAdd(&ws.Fnb[3 * jj + 2], -g1z);
-                    atomicAdd(&ws.Fnb[3 * kk], -g2x); atomicAdd(&ws.Fnb[3 * kk + 1], -g2y); atomicAdd(&ws.Fnb[3 * kk + 2], -g2z);
-                    vr[0] -= (double)(g1x * d1.x + g2x * d2.x);
-                    vr[1] -= (double)(g1y * d1.y + g2y * d2.y);
-                    vr[2] -= (double)(g1z * d1.z + g2z * d2.z);
-                    vr[3] -= (double)(g1x * d1.y + g2x * d2.y);
-                    vr[4] -= (double)(g1y * d1.z + g2y * d2.z);
-                    vr[5] -= (double)(g1z * d1.x + g2z * d2.x);
+                    if (on) {
+                        atomicAdd(&ws.Fnb[3 * kk], -g2x);
+                        atomicAdd(&ws.Fnb[3 * kk + 1], -g2y);
+                        atomicAdd(&ws.Fnb[3 * kk + 2], -g2z);
+                    }
+                    /* j side: sum each run of equal j, one atomic per run */
+#pragma unroll
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const float ox = __shfl_down_sync(FULLM, g1x, off), oy = __shfl_down_sync(FULLM, g1y, off),
+                                    oz = __shfl_down_sync(FULLM, g1z, off);
+                        const int ok = __shfl_down_sync(FULLM, jj, off);
+                        if (lane + off < 32 && ok == jj) {
+                            g1x += ox;
+                            g1y += oy;
+                            g1z += oz;
+                        }
+                    }
+                    const int prev = __shfl_up_sync(FULLM, jj, 1);
+                    if (t < hi && (lane == 0 || prev != jj)) {
+                        atomicAdd(&ws.Fnb[3 * jj], -g1x);
+                        atomicAdd(&ws.Fnb[3 * jj + 1], -g1y);
+                        atomicAdd(&ws.Fnb[3 * jj + 2], -g1z);
+                    }
                 }
                 __syncwarp();
                 if (whole || row >= na) break;
             }
         }
+    /* virial of atom i's energy: every neighbour force Fnb[t] (pairs and
+     * triplets) times its displacement, summed in FP64 -- the same sum as
+     * -(dE/dd) (x) d taken term by term, formed once per neighbour */
+    for (int t = lane; t < n; t += 32) {
+        const float4 d = ws.d[t];
+        const double fx = ws.Fnb[3 * t], fy = ws.Fnb[3 * t + 1], fz = ws.Fnb[3 * t + 2];
+        vr[0] += fx * d.x; vr[1] += fy * d.y; vr[2] += fz * d.z;
+        vr[3] += fx * d.y; vr[4] += fy * d.z; vr[5] += fz * d.x;
+    }
     /* gather: atom i and its neighbours into the structure's force array */
     fi0 = bsumf(fi0);
     fi1 = bsumf(fi1);
@@ -560,6 +631,47 @@ __device__ double evaluate(const BArgs &A, BShared &sh, const double *dof, doubl
     }
     const int w0 = 2 * nq[0] + 1, w1 = 2 * nq[1] + 1, w2 = 2 * nq[2] + 1, nimg = w0 * w1 * w2;
     const double rc2 = P.rc * P.rc;
+    if (nimg <= 32 * BIMG) {
+        /* each lane holds the Cartesian shifts of images lane, lane+32, ...;
+         * candidates in the order (j, image), as the general loop below */
+        double shx[BIMG], shy[BIMG], shz[BIMG];
+        unsigned zero = 0; /* bit t: image lane + 32 t is the unshifted cell */
+#pragma unroll
+        for (int t = 0; t < BIMG; t++) {
+            const int im = lane + 32 * t;
+            const int c2 = im % w2 - nq[2], u = im / w2, c1 = u % w1 - nq[1], c0 = u / w1 - nq[0];
+            shx[t] = c0 * sh.L[0] + c1 * sh.L[3] + c2 * sh.L[6];
+            shy[t] = c0 * sh.L[1] + c1 * sh.L[4] + c2 * sh.L[7];
+            shz[t] = c0 * sh.L[2] + c1 * sh.L[5] + c2 * sh.L[8];
+            if (c0 == 0 && c1 == 0 && c2 == 0) zero |= 1u << t;
+        }
+        for (int i = w; i < N; i += BWARPS) {
+            int count = 0;
+            const double xi0 = sh.xc[3 * i], xi1 = sh.xc[3 * i + 1], xi2 = sh.xc[3 * i + 2];
+            for (int j = 0; j < N; j++) {
+                const double b0 = sh.xc[3 * j] - xi0, b1 = sh.xc[3 * j + 1] - xi1, b2 = sh.xc[3 * j + 2] - xi2;
+#pragma unroll
+                for (int t = 0; t < BIMG; t++) {
+                    if (32 * t >= nimg) break;
+                    const int im = lane + 32 * t;
+                    const double d0 = b0 + shx[t], d1 = b1 + shy[t], d2 = b2 + shz[t];
+                    const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+                    const bool ok = im < nimg && r2 < rc2 && !(j == i && ((zero >> t) & 1u));
+                    const unsigned m = __ballot_sync(FULLM, ok);
+                    const int pos = count + __popc(m & ((1u << lane) - 1u));
+                    if (ok && pos < BMAXNB) {
+                        nbj[i * BMAXNB + pos] = j;
+                        nbd[i * BMAXNB + pos] = make_float4((float)d0, (float)d1, (float)d2, (float)sqrt(r2));
+                    }
+                    count += __popc(m);
+                }
+            }
+            if (lane == 0) {
+                sh.nn[i] = count < BMAXNB ? count : BMAXNB;
+                if (count > BMAXNB) sh.flag = 2;
+            }
+        }
+    } else
     for (int i = w; i < N; i += BWARPS) {
         int count = 0;
         const double xi0 = sh.xc[3 * i], xi1 = sh.xc[3 * i + 1], xi2 = sh.xc[3 * i + 2];
@@ -698,8 +810,8 @@ __global__ void __launch_bounds__(BWARPS * 32) k_relax_batch(BArgs A) {
     for (;;) {
         if (tid == 0) sh.s = atomicAdd(A.queue, 1);
         __syncthreads();
-        const int s = sh.s;
-        if (s >= A.S) break;
+        if (sh.s >= A.S) break;
+        const int s = A.order[sh.s];
         const int N = A.nat[s], o = A.off[s], rlxt = A.rlxt;
         const int n = 3 * N + (rlxt == 3 ? 9 : 0);
         if (tid == 0) {
@@ -931,6 +1043,7 @@ static int build_bparams(const mb_model *m, BParams *B, float **w_out, size_t *w
         B->zeta[z] = (float)P.zeta[z];
         B->powz[z] = (float)P.powz[z];
         B->zbits[z] = z < P.nz ? P.zbits[z] : 0;
+        B->zstd = P.zeta_std;
         B->zm1bits[z] = z < P.nz ? P.zm1bits[z] : 0;
     }
     for (int l = 0; l < MB_MAXL; l++) B->lam[l] = (float)P.lam[l];
@@ -948,7 +1061,7 @@ static int build_bparams(const mb_model *m, BParams *B, float **w_out, size_t *w
 }
 
 extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const int *d_off, const int *d_spc,
-                               double *d_lat, double *d_x, double p_ev, double urep, int rlxt, int mitr, double fmax,
+                               const int *d_order, double *d_lat, double *d_x, double p_ev, double urep, int rlxt, int mitr, double fmax,
                                double *d_H, int *d_iters, int *d_status, void *stream, long long *evals_out,
                                float *ms_out) {
     cudaStream_t st = (cudaStream_t)stream;
@@ -989,7 +1102,7 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
         BArgs a;
         a.S = S; a.rlxt = rlxt; a.mitr = mitr;
         a.p_ev = p_ev; a.urep = urep; a.fmax = fmax; a.sigma = 0.1;
-        a.nat = d_nat; a.off = d_off; a.spc = d_spc;
+        a.nat = d_nat; a.off = d_off; a.spc = d_spc; a.order = d_order;
         a.lat = d_lat; a.x = d_x; a.H = d_H; a.iters = d_iters; a.status = d_status;
         a.P = dp; a.W = dw; a.queue = queue; a.hmat = hm; a.nbd = nbd; a.nbj = nbj; a.evals = evals;
         cudaEventRecord(e0, st);

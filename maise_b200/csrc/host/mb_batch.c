@@ -22,8 +22,8 @@ void mb_handle_set_batch_stats(mb_potential *p, long long evals, float ms);
 
 int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, double *lat, double *x, double p_gpa,
                    double urep, int rlxt, int mitr, double fmax, double *H, int *iters, int *status) {
-    int *off, total = 0, s, rc = MB_OK;
-    int *d_nat = NULL, *d_off = NULL, *d_spc = NULL, *d_iters = NULL, *d_status = NULL;
+    int *off, *order, total = 0, s, rc = MB_OK;
+    int *d_nat = NULL, *d_off = NULL, *d_spc = NULL, *d_iters = NULL, *d_status = NULL, *d_order = NULL;
     double *d_lat = NULL, *d_x = NULL, *d_H = NULL;
     long long evals = 0;
     float ms = 0.0f;
@@ -49,6 +49,15 @@ int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, do
             free(off);
             return mb_handle_fail(MB_ERR_ARG, "species index out of range");
         }
+    /* the persistent CTAs take structures largest first, so that the last
+     * ones to start are small and the population finishes evenly */
+    order = (int *)malloc(sizeof(int) * S);
+    {
+        int n, k = 0;
+        for (n = 64; n >= 1; n--)
+            for (s = 0; s < S; s++)
+                if (nat[s] == n) order[k++] = s;
+    }
     cudaSetDevice(mb_handle_device(pot));
     st = mb_handle_stream(pot);
     e = cudaMalloc((void **)&d_nat, sizeof(int) * S);
@@ -59,6 +68,8 @@ int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, do
     if (!e) e = cudaMalloc((void **)&d_lat, sizeof(double) * 9 * S);
     if (!e) e = cudaMalloc((void **)&d_x, sizeof(double) * 3 * total);
     if (!e) e = cudaMalloc((void **)&d_H, sizeof(double) * S);
+    if (!e) e = cudaMalloc((void **)&d_order, sizeof(int) * S);
+    if (!e) e = cudaMemcpyAsync(d_order, order, sizeof(int) * S, cudaMemcpyHostToDevice, (cudaStream_t)st);
     if (!e) e = cudaMemcpyAsync(d_nat, nat, sizeof(int) * S, cudaMemcpyHostToDevice, (cudaStream_t)st);
     if (!e) e = cudaMemcpyAsync(d_off, off, sizeof(int) * (S + 1), cudaMemcpyHostToDevice, (cudaStream_t)st);
     if (!e) e = cudaMemcpyAsync(d_spc, atmn, sizeof(int) * total, cudaMemcpyHostToDevice, (cudaStream_t)st);
@@ -68,7 +79,7 @@ int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, do
         rc = mb_handle_fail(MB_ERR_CUDA, cudaGetErrorString(e));
         goto out;
     }
-    e = (cudaError_t)mbk_relax_batch(m, S, d_nat, d_off, d_spc, d_lat, d_x, p_gpa / MB_EV2GPA, urep > 0 ? urep : 0.0,
+    e = (cudaError_t)mbk_relax_batch(m, S, d_nat, d_off, d_spc, d_order, d_lat, d_x, p_gpa / MB_EV2GPA, urep > 0 ? urep : 0.0,
                                      rlxt, mitr, fmax, d_H, d_iters, d_status, st, &evals, &ms);
     if (e == cudaErrorInvalidValue) {
         rc = mb_handle_fail(MB_ERR_MODEL, "batched relax needs a basis with <= 7 G4 exponents, zeta in {integers}, "
@@ -88,7 +99,8 @@ int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, do
     mb_handle_set_batch_stats(pot, evals, ms);
 out:
     cudaFree(d_nat); cudaFree(d_off); cudaFree(d_spc); cudaFree(d_iters); cudaFree(d_status);
-    cudaFree(d_lat); cudaFree(d_x); cudaFree(d_H);
+    cudaFree(d_lat); cudaFree(d_x); cudaFree(d_H); cudaFree(d_order);
     free(off);
+    free(order);
     return rc;
 }

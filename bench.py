@@ -162,6 +162,139 @@ def cpu_baseline(w, model_dir, max_seconds=40.0):
                       f"{t_first:.1f} s incl. allocation, excluded); median {per:.3f} s per call"}
 
 
+POP_WORKLOAD = ("EA population relax: 256 Mg-Ca structures of 8-64 atoms, 20 A^3/atom +-15%, angles 60-120 deg, "
+                "2.0 A minimum distance, random compositions; 145-10-10-1 tanh model; RLXT 3 (positions and cell) "
+                "to max |F| < 0.01 eV/A, UREP 100 eV")
+GEN_WORKLOAD = ("surrogate-screened EA generation: 4096 Cu-Pd-Ag offspring of 16-48 atoms generated as the "
+                "population relax; 128-bin per-pair histograms -> 768-128-64-64-1 SiLU FP32 MLP trained by Adam on "
+                "20000 relaxed offspring; the best 25% by prediction are relaxed")
+
+
+def _binding_model(td, name, structures, spcz, seed, angular=0.3):
+    from maise_b200 import models
+
+    big = max(structures, key=lambda s: len(s["atmn"]))
+    path = os.path.join(td, name)
+    os.makedirs(path, exist_ok=True)
+    models.random_model(os.path.join(path, "model"), list(spcz), models.Basis(), (big["X"], big["LAT"], big["atmn"], 3),
+                        seed=seed, binding=True, angular=angular)
+    return os.path.join(path, "model")
+
+
+def population_relax(local, td, plain_sample=16, mitr=1000, fmax=0.01, urep=100.0):
+    """Relaxed structures/s of the persistent batched relax (FP32 descriptors
+    and MLP, FP64 reductions and BFGS) against the plain one-structure FP64
+    path (host BFGS over the GPU E/F/S) on a sample of the same population;
+    every batched minimum is re-evaluated by the FP64 path."""
+    import maise_b200
+    from maise_b200 import workloads
+
+    pop = workloads.ea_population(count=256, seed=3)
+    nat = np.array([len(s["atmn"]) for s in pop])
+    pot = maise_b200.Potential(_binding_model(td, "pop", pop, (12, 20), 5), device=local)
+    pot.relax_batch(pop[:4], urep=urep, rlxt=3, mitr=3, fmax=fmax)  # module load, launch set-up
+    t0 = time.perf_counter()
+    rb = pot.relax_batch(pop, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
+    wall = time.perf_counter() - t0
+    dE, f64 = [], []
+    for k, s in enumerate(pop):
+        r = pot.efs(rb["X"][k], rb["LAT"][k], s["atmn"], ND=3, NM=300, urep=urep)
+        dE.append(abs(rb["H"][k] - r["H"]) / nat[k])
+        f64.append(float(np.abs(r["F"]).max()))
+    dE, f64 = np.array(dE), np.array(f64)
+    conv = rb["status"] == 0
+    t0 = time.perf_counter()
+    plain = [pot.relax_fmax(s["X"], s["LAT"], s["atmn"], ND=3, NM=300, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
+             for s in pop[:plain_sample]]
+    t_plain = time.perf_counter() - t0
+    batched = len(pop) / (rb["ms"] / 1e3)
+    plain_sps = plain_sample / t_plain
+    pot.close()
+    return {"workload": POP_WORKLOAD, "structures": len(pop), "atoms": int(nat.sum()),
+            "batched_structures_per_s": batched, "batched_e2e_structures_per_s": len(pop) / wall,
+            "plain_structures_per_s": plain_sps, "speedup_vs_plain": batched / plain_sps,
+            "plain_sample": f"first {plain_sample} structures of the population, one mb_relax_fmax each",
+            "batched_converged": int(conv.sum()), "plain_converged": int(sum(r["converged"] for r in plain)),
+            "batched_evals": rb["evals"], "kernel_ms": rb["ms"],
+            "fp32_vs_fp64_ev_per_atom_max_converged": float(dE[conv].max()) if conv.any() else None,
+            "fp64_max_force_converged_ev_per_a": float(f64[conv].max()) if conv.any() else None,
+            "dtype": "descriptors/MLP fp32, reductions/BFGS fp64"}
+
+
+def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs=60, mitr=300, fmax=0.01,
+                         urep=100.0):
+    """One EA generation with and without the surrogate screen: relax every
+    offspring, or predict all, keep the best quarter and relax those; the
+    full relaxation of every offspring judges the screen's recall of the
+    best 10%.  Training pairs come from relaxing 20000 other offspring."""
+    import maise_b200
+    from maise_b200 import workloads
+    from maise_b200.surrogate import Surrogate, keep_best, recall
+
+    spc = (29, 46, 47)
+    train = workloads.ea_population(count=n_train, nmin=16, nmax=48, seed=11, species=spc)
+    gen = workloads.ea_population(count=n_gen, nmin=16, nmax=48, seed=12, species=spc)
+    pot = maise_b200.Potential(_binding_model(td, "gen", train, spc, 5), device=local)
+    t0 = time.perf_counter()
+    rt = pot.relax_batch(train, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
+    t_data = time.perf_counter() - t0
+    y = rt["H"] / np.array([len(s["atmn"]) for s in train])
+    sur = Surrogate(3, device=local)
+    t0 = time.perf_counter()
+    feat = sur.features(train)
+    loss = sur.fit(feat, y, epochs=epochs, batch=256, lr=1e-3)
+    t_fit = time.perf_counter() - t0
+    nat = np.array([len(s["atmn"]) for s in gen])
+    t0 = time.perf_counter()
+    ra = pot.relax_batch(gen, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
+    t_all = time.perf_counter() - t0
+    truth = ra["H"] / nat
+    t0 = time.perf_counter()
+    pred = sur.screen(gen)
+    kept = keep_best(pred, keep)
+    pot.relax_batch([gen[i] for i in kept], urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
+    t_scr = time.perf_counter() - t0
+    e0 = np.array([pot.energy(s["X"], s["LAT"], s["atmn"], ND=3, NM=300, urep=urep)["H"] for s in gen]) / nat
+    sur.close()
+    pot.close()
+    return {"workload": GEN_WORKLOAD, "offspring": n_gen, "train_pairs": n_train, "keep": keep,
+            "recall_top10": recall(pred, truth, keep), "recall_top10_by_unrelaxed_energy": recall(e0, truth, keep),
+            "recall_top10_random_expectation": keep,
+            "generation_s_relax_all": t_all, "generation_s_screened": t_scr, "speedup": t_all / t_scr,
+            "train_data_relax_s": t_data, "fit_s": t_fit, "epochs": epochs, "final_loss": float(loss[-1]),
+            "judge": "batched relax of every offspring (FP32 descriptors/MLP, FP64 BFGS)"}
+
+
+def profile_case(case):
+    """Small cases sized for an ncu capture (a few MB on the device):
+    md           the 4000-atom workload, 3 + 3 NVT steps (k_efs launches)
+    relax-batch  64 Mg-Ca structures of the population relax, 20 BFGS iterations
+    surrogate    features of 512 Cu-Pd-Ag offspring and 5 training epochs"""
+    import maise_b200
+    from maise_b200 import atomic_mass, maxwell, workloads
+
+    td = tempfile.mkdtemp()
+    if case == "md":
+        w, basis = workload()
+        pot = maise_b200.Potential(make_model(td, w, basis))
+        V = maxwell([atomic_mass(w["spcz"][s]) for s in w["atmn"]], 600.0, seed=7)
+        st = pot.md_nvt(w["X"], w["LAT"], w["atmn"], V, 600.0, nsteps=3, NM=100, trace=False)
+        pot.md_nvt(st["X"], w["LAT"], w["atmn"], st["V"], 600.0, nsteps=3, NM=100, xi=st["xi"], trace=False)
+    elif case == "relax-batch":
+        pop = workloads.ea_population(count=64, seed=3)
+        pot = maise_b200.Potential(_binding_model(td, "pop", pop, (12, 20), 5))
+        r = pot.relax_batch(pop, urep=100.0, rlxt=3, mitr=20, fmax=0.01)
+        print(f"relax-batch: {r['evals']} evaluations in {r['ms']:.1f} ms")
+    else:
+        from maise_b200.surrogate import Surrogate
+
+        pop = workloads.ea_population(count=512, nmin=16, nmax=48, seed=11, species=(29, 46, 47))
+        sur = Surrogate(3)
+        feat = sur.features(pop)
+        sur.fit(feat, np.linspace(-4.0, -3.0, len(pop)), epochs=5, batch=256)
+        sur.screen(pop)
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference CPU implementation on the same workload."""
     from oracle import RefOracle, ref_available
@@ -210,6 +343,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--no-population", action="store_true", help="skip the population relax and surrogate legs")
+    ap.add_argument("--profile-case", choices=["md", "relax-batch", "surrogate"],
+                    help="run one small case of a hot kernel for an ncu capture and exit (no bench line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -226,6 +362,9 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         if dist is not None:
@@ -326,6 +465,9 @@ def main():
             "e2e": e2e, "roofline": roof, "gpu_launches": launches, "clocks": clocks}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, td)
+    if rank == 0 and not args.no_population:
+        line["population_relax"] = population_relax(local, td)
+        line["surrogate_generation"] = surrogate_generation(local, td)
     if rank == 0:
         print(json.dumps(line))
     pot.close()

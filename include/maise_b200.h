@@ -168,11 +168,14 @@ int mb_efs_noalloc(mb_potential *pot, int N, int NM, int ND, const double *lat9,
 
 /* ---- diagnostics (no counterpart in the reference) ---- */
 
-/* Run the NVT loop of mb_md_nvt as CUDA graphs (enable=1, the default; the
- * environment variable MAISE_B200_GRAPHS=0 makes 0 the default) or as plain
- * launches (0).  Each chunk of 10 steps is captured once and replayed while
- * the buffers, sizes and step parameters it was captured for hold; results
- * are the same either way. */
+/* Replay captured CUDA graphs (enable=1, the default; the environment
+ * variable MAISE_B200_GRAPHS=0 makes 0 the default) or issue plain launches
+ * (0).  Graphs are used for the NVT loop of mb_md_nvt (chunks of 10 steps)
+ * and for every single-structure pass (mb_efs, mb_energy, CALL_MAISE and
+ * each evaluation of mb_relax / mb_relax_fmax: wrap, list, descriptor pass,
+ * finalize and the result copies in one launch, the cell updated in place).
+ * A graph is captured once and replayed while the buffers and sizes it was
+ * captured for hold; results are the same either way. */
 int mb_graphs(mb_potential *p, int enable);
 
 /* Start (enable=1) or stop timing of the fused descriptor/force kernel: every

@@ -73,12 +73,12 @@ struct BArgs {
 struct WarpWS {
     float4 d[BMAXNB];
     float ir[BMAXNB], fa[BMAXNB], fb[BMAXNB];
-    float P[BMAXNB * BNE];
+    alignas(16) float P[BMAXNB * 8]; /* exp(-eta r^2) per neighbour, BNE used of 8 */
     float Fnb[BMAXNB * 3];
-    float grid[BCELLS];
+    alignas(16) float grid[BCELLS];
     float G[BMAXD];
     float h[4 * MB_MAXH];
-    double red[64];
+    float red[64];
     int j[BMAXNB], sp[BMAXNB], raw[BMAXNB];
     unsigned tl[BTL];
     int blk[6][2];
@@ -287,7 +287,7 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
         ws.fa[t] = fa;
         ws.fb[t] = fcutf(P.f_rc4[p], r);
 #pragma unroll
-        for (int e = 0; e < BNE; e++) ws.P[t * BNE + e] = e < P.ne ? expf(-P.f_eta4[p][e] * r * r) : 0.0f;
+        for (int e = 0; e < 8; e++) ws.P[t * 8 + e] = e < P.ne ? expf(-P.f_eta4[p][e] * r * r) : 0.0f;
         if (r < P.f_rc2[p]) {
 #pragma unroll
             for (int f = 0; f < 16; f++) {
@@ -325,6 +325,15 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
             for (int k = 0; k < BCELLS; k++) acc[k] = 0.0f;
             const int na = ws.seg[a], nb = ws.seg[b], oa = ws.seg[4 + a], ob = ws.seg[4 + b];
             int row = 0, start = tl_pos;
+            /* j and k species are fixed within the block: hoist their parameters */
+            const int sja = (a + s0) % ns, skb = (b + s0) % ns;
+            const int p01 = s0 * s0 + sja * sja, p02 = s0 * s0 + skb * skb, p12 = sja * sja + skb * skb;
+            const float rc2_01 = P.f_rc2[p01], rc4_01 = P.f_rc4[p01], rc4_02 = P.f_rc4[p02];
+            const float rc4sq_12 = P.f_rc4sq[p12], rc4_12 = P.f_rc4[p12];
+            const float drc4 = P.d_rc4, drc4sq = P.d_rc4sq;
+            float eta12[BNE];
+#pragma unroll
+            for (int e = 0; e < BNE; e++) eta12[e] = P.f_eta4[p12][e];
             for (;;) {
                 int from = tl_pos;
                 for (; row < na; row++) {
@@ -333,7 +342,13 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
                     for (int kb = k0; kb < nb; kb += 32) {
                         int kk = ob + kb + lane;
                         bool ok = false;
-                        if (kb + lane < nb) ok = tgate(P, ws, s0, jj, kk);
+                        if (kb + lane < nb) {
+                            const float4 d1 = ws.d[jj], d2 = ws.d[kk];
+                            const float dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+                            const float r3s = dx * dx + dy * dy + dz * dz;
+                            ok = (d1.w < rc2_01 && d1.w < rc4_01 && d2.w < rc4_02 && r3s < rc4sq_12) ||
+                                 (d1.w < drc4 && d2.w < drc4 && r3s < drc4sq);
+                        }
                         unsigned m = __ballot_sync(FULLM, ok);
                         if (ok) ws.tl[tl_pos + __popc(m & ((1u << lane) - 1u))] = (unsigned)jj | ((unsigned)kk << 16);
                         tl_pos += __popc(m);
@@ -344,19 +359,21 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
                     unsigned pk = ws.tl[t];
                     int jj = pk & 0xffff, kk = pk >> 16;
                     float4 d1 = ws.d[jj], d2 = ws.d[kk];
-                    int sj = ws.sp[jj], sk = ws.sp[kk], p12 = sj * sj + sk * sk;
-                    int p01 = s0 * s0 + sj * sj, p02 = s0 * s0 + sk * sk;
                     float dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
                     float r3s = dx * dx + dy * dy + dz * dz, r3 = sqrtf(r3s);
-                    if (!(d1.w < P.f_rc2[p01] && d1.w < P.f_rc4[p01] && d2.w < P.f_rc4[p02] && r3s < P.f_rc4sq[p12]))
-                        continue;
+                    if (!(d1.w < rc2_01 && d1.w < rc4_01 && d2.w < rc4_02 && r3s < rc4sq_12)) continue;
                     float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ws.ir[jj] * ws.ir[kk]);
-                    float A3 = 2.0f * ws.fa[jj] * ws.fb[kk] * fcutf(P.f_rc4[p12], r3);
+                    float A3 = 2.0f * ws.fa[jj] * ws.fb[kk] * fcutf(rc4_12, r3);
                     float lz[BNZL];
                     angularf(P, c, lz, nullptr);
+                    const float4 *pj = reinterpret_cast<const float4 *>(ws.P + jj * 8);
+                    const float4 *pk4 = reinterpret_cast<const float4 *>(ws.P + kk * 8);
+                    const float4 ja = pj[0], jb = pj[1], ka = pk4[0], kb4 = pk4[1];
+                    const float pjk[8] = {ja.x * ka.x, ja.y * ka.y, ja.z * ka.z, ja.w * ka.w,
+                                          jb.x * kb4.x, jb.y * kb4.y, jb.z * kb4.z, jb.w * kb4.w};
 #pragma unroll
                     for (int e = 0; e < BNE; e++) {
-                        float ex = A3 * ws.P[jj * BNE + e] * ws.P[kk * BNE + e] * expf(-P.f_eta4[p12][e] * r3s);
+                        float ex = A3 * pjk[e] * expf(-eta12[e] * r3s);
 #pragma unroll
                         for (int zl = 0; zl < BNZL; zl++) acc[e * BNZL + zl] += ex * lz[zl];
                     }
@@ -375,7 +392,7 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
             __syncwarp();
             if (lane == 0) {
                 int base = P.ind4[a * a + b * b];
-                for (int f = 0; f < P.ng4; f++) ws.G[base + f] += (float)ws.red[P.g4_cell[f]];
+                for (int f = 0; f < P.ng4; f++) ws.G[base + f] += ws.red[P.g4_cell[f]];
             }
             __syncwarp();
         }
@@ -429,7 +446,7 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
         ws.fa[t] = f4;
         ws.fb[t] = df4;
 #pragma unroll
-        for (int q = 0; q < BNE; q++) ws.P[t * BNE + q] = q < P.ne ? expf(-P.d_eta4[q] * r * r) : 0.0f;
+        for (int q = 0; q < 8; q++) ws.P[t * 8 + q] = q < P.ne ? expf(-P.d_eta4[q] * r * r) : 0.0f;
         int ds1 = (ws.sp[t] - s0 + ns) % ns;
         const float *gg = ws.G + P.ind2[ds1];
         float cp = 0.0f;
@@ -458,6 +475,10 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
 
     /* reverse triplets, reusing the lists when they fit */
     blkid = 0;
+    const float drc4 = P.d_rc4, drc4sq = P.d_rc4sq;
+    float deta[BNE];
+#pragma unroll
+    for (int q = 0; q < BNE; q++) deta[q] = P.d_eta4[q];
     for (int a = 0; a < ns; a++)
         for (int b = a; b < ns; b++, blkid++) {
             const int base = P.ind4[a * a + b * b];
@@ -500,28 +521,35 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
                     float4 d1 = ws.d[jj], d2 = ws.d[kk];
                     float wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
                     float r3s = wx * wx + wy * wy + wz * wz, r3 = sqrtf(r3s);
-                    on = d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq;
+                    on = d1.w < drc4 && d2.w < drc4 && r3s < drc4sq;
                     if (on) {
                     float r1 = d1.w, r2 = d2.w, ir1 = ws.ir[jj], ir2 = ws.ir[kk], ir3 = 1.0f / r3;
                     float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
                     float f3, df3;
-                    fcutf_d(P.d_rc4, r3, f3, df3);
+                    fcutf_d(drc4, r3, f3, df3);
                     float f1 = ws.fa[jj], df1 = ws.fb[jj], f2 = ws.fa[kk], df2 = ws.fb[kk];
                     float lz[BNZL], lzp[BNZL];
                     angularf(P, c, lz, lzp);
                     float Q = 0.0f, Qe = 0.0f, Qc = 0.0f;
+                    const float4 *pj = reinterpret_cast<const float4 *>(ws.P + jj * 8);
+                    const float4 *pk4 = reinterpret_cast<const float4 *>(ws.P + kk * 8);
+                    const float4 ja = pj[0], jb = pj[1], ka = pk4[0], kb4 = pk4[1];
+                    const float pjk[8] = {ja.x * ka.x, ja.y * ka.y, ja.z * ka.z, ja.w * ka.w,
+                                          jb.x * kb4.x, jb.y * kb4.y, jb.z * kb4.z, jb.w * kb4.w};
+                    const float4 *g4 = reinterpret_cast<const float4 *>(ws.grid);
 #pragma unroll
                     for (int q = 0; q < BNE; q++) {
-                        float ex = ws.P[jj * BNE + q] * ws.P[kk * BNE + q] * expf(-P.d_eta4[q] * r3s);
+                        const float ex = pjk[q] * expf(-deta[q] * r3s);
+                        const float4 ga = g4[2 * q], gb = g4[2 * q + 1];
+                        const float cg[8] = {ga.x, ga.y, ga.z, ga.w, gb.x, gb.y, gb.z, gb.w};
                         float u = 0.0f, vv = 0.0f;
 #pragma unroll
                         for (int zl = 0; zl < BNZL; zl++) {
-                            float cg = ws.grid[q * BNZL + zl];
-                            u += cg * lz[zl];
-                            vv += cg * lzp[zl];
+                            u += cg[zl] * lz[zl];
+                            vv += cg[zl] * lzp[zl];
                         }
                         Q += ex * u;
-                        Qe += P.d_eta4[q] * ex * u;
+                        Qe += deta[q] * ex * u;
                         Qc += ex * vv;
                     }
                     float Af = 2.0f * f1 * f2 * f3;

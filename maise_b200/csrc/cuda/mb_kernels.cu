@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include "../mb_internal.h"
 
@@ -360,15 +361,19 @@ struct EfsSmem {
 #define MB_MAX_BLOCKS 6 /* species blocks (a<=b) for 3 species */
 
 __host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7; }
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+/* row stride of the per-neighbour exponential factors: even, so that rows
+ * start on 16 bytes (the neighbour capacity is a multiple of 8) */
+__host__ __device__ constexpr int nep(int ne) { return (ne + 1) & ~1; }
 
 __host__ __device__ inline size_t efs_smem_bytes(int cap, int D, int ne, int ng2, int nzl_cells, int warps, int tl) {
     size_t b = 0;
     b += align8(sizeof(int) * cap) * 3;           /* j, sp, raw_sp */
     b += sizeof(double4) * cap;                   /* d */
     b += sizeof(double) * cap * 3;                /* ir, fa, fb */
-    b += sizeof(double) * cap * ne;               /* P */
+    b += sizeof(double) * cap * nep(ne);          /* P */
     b += sizeof(double) * cap * 3;                /* Fnb */
-    b += sizeof(double) * D;                      /* G */
+    b += align16(sizeof(double) * D);             /* G */
     b += sizeof(double) * nzl_cells;              /* grid */
     b += sizeof(double) * warps * 64;             /* red */
     b += sizeof(double) * cap * (ng2 > 1 ? ng2 : 1); /* tmp */
@@ -387,9 +392,9 @@ __device__ inline EfsSmem efs_carve(char *base, int cap, int D, int ne, int ng2,
     s.ir = (double *)p; p += sizeof(double) * cap;
     s.fa = (double *)p; p += sizeof(double) * cap;
     s.fb = (double *)p; p += sizeof(double) * cap;
-    s.P = (double *)p; p += sizeof(double) * cap * ne;
+    s.P = (double *)p; p += sizeof(double) * cap * nep(ne);
     s.Fnb = (double *)p; p += sizeof(double) * cap * 3;
-    s.G = (double *)p; p += sizeof(double) * D;
+    s.G = (double *)p; p += align16(sizeof(double) * D);
     s.grid = (double *)p; p += sizeof(double) * nzl_cells;
     s.red = (double *)p; p += sizeof(double) * warps * 64;
     s.tmp = (double *)p; p += sizeof(double) * cap * (ng2 > 1 ? ng2 : 1);
@@ -493,22 +498,44 @@ __device__ __forceinline__ void run_list(const EfsSmem &s, int from, int to, int
     }
 }
 
+/* body(jj, kk, valid) with the whole warp on every round (for bodies that
+ * exchange values across lanes); lanes past the end get valid = false and
+ * jj = -1 - lane, so equal jj values stay adjacent */
+template <class Body>
+__device__ __forceinline__ void run_list_all(const EfsSmem &s, int from, int to, int lane, Body body) {
+    for (int base = from; base < to; base += 32) {
+        const int t = base + lane;
+        if (t < to) {
+            const unsigned pk = s.tl[t];
+            body((int)(pk & 0xffffu), (int)(pk >> 16), true);
+        } else {
+            body(-1 - lane, 0, false);
+        }
+    }
+}
+
 /* Enumerate block (a,b) for this warp and process it, reusing the list
  * entries [blk[0], blk[1]) when `reuse` and filling (in rounds when the
  * region overflows) otherwise.  Records the range for later reuse and
  * returns 0 if the region overflowed (then the range is not reusable). */
-template <int WPA, class Accept, class Body>
+template <int WPA, bool ALL = false, class Accept, class Body>
 __device__ __forceinline__ int for_block(const EfsSmem &s, int a, int b, int *blk, int reuse, int &pos, int lo,
                                          int hi, int warp, int lane, Accept accept, Body body) {
     if (reuse) {
-        run_list(s, blk[0], blk[1], lane, body);
+        if constexpr (ALL)
+            run_list_all(s, blk[0], blk[1], lane, body);
+        else
+            run_list(s, blk[0], blk[1], lane, body);
         return 1;
     }
     int start = pos, row = warp, whole = 1;
     for (;;) {
         const int from = pos;
         row = fill_rows<WPA>(s, a, b, row, pos, hi, lane, accept);
-        run_list(s, from, pos, lane, body);
+        if constexpr (ALL)
+            run_list_all(s, from, pos, lane, body);
+        else
+            run_list(s, from, pos, lane, body);
         __syncwarp();
         if (row >= s.seg[a]) break;
         whole = 0; /* region full: restart it for the next round */
@@ -523,6 +550,7 @@ template <int NE, int NZ, int NLAM, int WPA, int APB>
 __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
     constexpr int NZL = NZ * NLAM;
     constexpr int WARPS = WPA;
+    constexpr int NEP = nep(NE);
     extern __shared__ __align__(16) char smem_raw[];
     __shared__ mb_params Ps;
     {
@@ -595,8 +623,8 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
         s.fa[t] = fa;
         s.fb[t] = fcut(P.f_rc4[p], r);
 #pragma unroll
-        for (int e = 0; e < NE; e++)
-            if (e < ne) s.P[t * NE + e] = exp(-P.f_eta4[p][e] * r * r);
+        for (int e = 0; e < NEP; e++)
+            s.P[t * NEP + e] = e < ne ? exp(-P.f_eta4[p][e] * r * r) : 0.0;
         bool gate = r < P.f_rc2[p];
         for (int f = 0; f < ng2; f++) {
             double x = r - P.f_rs[p][f];
@@ -629,32 +657,51 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
                 double acc[CELLS];
 #pragma unroll
                 for (int k = 0; k < CELLS; k++) acc[k] = 0.0;
+                /* the species of j and k are fixed within the block (neighbours are
+                 * sorted by species relative to s0): hoist their parameters */
+                const int sja = (a + s0) % ns, skb = (b + s0) % ns;
+                const int p01 = s0 * s0 + sja * sja, p02 = s0 * s0 + skb * skb, p12 = sja * sja + skb * skb;
+                const double rc2_01 = P.f_rc2[p01], rc4_01 = P.f_rc4[p01], rc4_02 = P.f_rc4[p02];
+                const double rc4sq_12 = P.f_rc4sq[p12], rc4_12 = P.f_rc4[p12];
+                const double drc4 = P.d_rc4, drc4sq = P.d_rc4sq;
+                auto accept_blk = [&](int jj, int kk) -> bool {
+                    const double4 d1 = s.d[jj], d2 = s.d[kk];
+                    const double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+                    const double r3s = dx * dx + dy * dy + dz * dz;
+                    return (d1.w < rc2_01 && d1.w < rc4_01 && d2.w < rc4_02 && r3s < rc4sq_12) ||
+                           (d1.w < drc4 && d2.w < drc4 && r3s < drc4sq);
+                };
+                const double *eta12 = P.f_eta4[p12];
                 auto body = [&](int jj, int kk) {
                     double4 d1 = s.d[jj], d2 = s.d[kk];
-                    int sj = s.sp[jj], sk = s.sp[kk];
-                    int p01 = s0 * s0 + sj * sj, p02 = s0 * s0 + sk * sk, p12 = sj * sj + sk * sk;
                     double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
                     double r3s = dx * dx + dy * dy + dz * dz;
-                    if (!(d1.w < P.f_rc2[p01] && d1.w < P.f_rc4[p01] && d2.w < P.f_rc4[p02] && r3s < P.f_rc4sq[p12]))
-                        return;
+                    if (!(d1.w < rc2_01 && d1.w < rc4_01 && d2.w < rc4_02 && r3s < rc4sq_12)) return;
                     nacc++;
                     double r3 = sqrt(r3s);
                     double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (s.ir[jj] * s.ir[kk]);
-                    double A3 = 2.0 * s.fa[jj] * s.fb[kk] * fcut(P.f_rc4[p12], r3);
+                    double A3 = 2.0 * s.fa[jj] * s.fb[kk] * fcut(rc4_12, r3);
                     double lz[NZL];
 #pragma unroll
                     for (int k = 0; k < NZL; k++) lz[k] = 0.0;
                     angular<NZ, NLAM>(P, c, lz, nullptr);
+                    const double2 *pj = reinterpret_cast<const double2 *>(s.P + jj * NEP);
+                    const double2 *pk = reinterpret_cast<const double2 *>(s.P + kk * NEP);
 #pragma unroll
-                    for (int e = 0; e < NE; e++) {
-                        if (e >= ne) break;
-                        double ex = A3 * s.P[jj * NE + e] * s.P[kk * NE + e] * exp(-P.f_eta4[p12][e] * r3s);
+                    for (int h = 0; h < NEP / 2; h++) {
+                        const double2 x = pj[h], y = pk[h];
 #pragma unroll
-                        for (int zl = 0; zl < NZL; zl++) acc[e * NZL + zl] += ex * lz[zl];
+                        for (int q = 0; q < 2; q++) {
+                            const int e = 2 * h + q;
+                            if (e >= NE || e >= ne) break;
+                            const double ex = A3 * (q ? x.y * y.y : x.x * y.x) * exp(-eta12[e] * r3s);
+#pragma unroll
+                            for (int zl = 0; zl < NZL; zl++) acc[e * NZL + zl] += ex * lz[zl];
+                        }
                     }
                 };
                 int *blk = s.blk + (blkid * WPA + warp) * 2;
-                tl_whole &= for_block<WPA>(s, a, b, blk, 0, tl_pos, tl_lo, tl_hi, warp, lane, accept_union, body);
+                tl_whole &= for_block<WPA>(s, a, b, blk, 0, tl_pos, tl_lo, tl_hi, warp, lane, accept_blk, body);
                 group_sync<WPA>();
 #pragma unroll
                 for (int ch = 0; ch < CELLS / 64; ch++) {
@@ -738,8 +785,8 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
         s.fa[t] = f4;
         s.fb[t] = df4;
 #pragma unroll
-        for (int e = 0; e < NE; e++)
-            if (e < ne) s.P[t * NE + e] = exp(-P.d_eta4[e] * r * r);
+        for (int e = 0; e < NEP; e++)
+            s.P[t * NEP + e] = e < ne ? exp(-P.d_eta4[e] * r * r) : 0.0;
         int ds1 = (s.sp[t] - s0 + ns) % ns;
         const double *g = s.G + P.ind2[ds1];
         double cpair = 0.0;
@@ -752,8 +799,6 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
         double v0 = cr * d.x, v1 = cr * d.y, v2 = cr * d.z;
         fi[0] += v0; fi[1] += v1; fi[2] += v2;
         s.Fnb[3 * t] = -v0; s.Fnb[3 * t + 1] = -v1; s.Fnb[3 * t + 2] = -v2;
-        vr[0] -= v0 * d.x; vr[1] -= v1 * d.y; vr[2] -= v2 * d.z;
-        vr[3] -= v0 * d.y; vr[4] -= v1 * d.z; vr[5] -= v2 * d.x;
         if (A.urep > 0.0) {
             double R = P.rm[s0] + P.rm[s.sp[t]];
             if (r < R) {
@@ -783,11 +828,15 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
                     for (int f = 0; f < P.ng4; f++)
                         s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam] += s.G[base + f];
                 group_sync<WPA>();
-                auto body = [&](int jj, int kk) {
+                auto body = [&](int jj, int kk, bool valid) {
+                    double g1x = 0.0, g1y = 0.0, g1z = 0.0, g2x = 0.0, g2y = 0.0, g2z = 0.0;
+                    bool on = false;
+                    if (valid) {
                     double4 d1 = s.d[jj], d2 = s.d[kk];
                     double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
                     double r3s = wx * wx + wy * wy + wz * wz;
-                    if (!(d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq)) return;
+                    on = d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq;
+                    if (on) {
                     double r3 = sqrt(r3s);
                     double r1 = d1.w, r2 = d2.w, ir1 = s.ir[jj], ir2 = s.ir[kk], ir3 = 1.0 / r3;
                     double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
@@ -798,21 +847,28 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
 #pragma unroll
                     for (int k = 0; k < NZL; k++) { lz[k] = 0.0; lzp[k] = 0.0; }
                     angular<NZ, NLAM>(P, c, lz, lzp);
+                    const double2 *pj = reinterpret_cast<const double2 *>(s.P + jj * NEP);
+                    const double2 *pk = reinterpret_cast<const double2 *>(s.P + kk * NEP);
                     double Q = 0.0, Qe = 0.0, Qc = 0.0;
 #pragma unroll
-                    for (int e = 0; e < NE; e++) {
-                        if (e >= ne) break;
-                        double ex = s.P[jj * NE + e] * s.P[kk * NE + e] * exp(-P.d_eta4[e] * r3s);
-                        double u = 0.0, v = 0.0;
+                    for (int h = 0; h < NEP / 2; h++) {
+                        const double2 x = pj[h], y = pk[h];
 #pragma unroll
-                        for (int zl = 0; zl < NZL; zl++) {
-                            double cg = s.grid[e * NZL + zl];
-                            u += cg * lz[zl];
-                            v += cg * lzp[zl];
+                        for (int q = 0; q < 2; q++) {
+                            const int e = 2 * h + q;
+                            if (e >= NE || e >= ne) break;
+                            const double ex = (q ? x.y * y.y : x.x * y.x) * exp(-P.d_eta4[e] * r3s);
+                            double u = 0.0, v = 0.0;
+#pragma unroll
+                            for (int zl = 0; zl < NZL; zl += 2) {
+                                const double2 cg = *reinterpret_cast<const double2 *>(s.grid + e * NZL + zl);
+                                u += cg.x * lz[zl] + cg.y * lz[zl + 1];
+                                v += cg.x * lzp[zl] + cg.y * lzp[zl + 1];
+                            }
+                            Q += ex * u;
+                            Qe += P.d_eta4[e] * ex * u;
+                            Qc += ex * v;
                         }
-                        Q += ex * u;
-                        Qe += P.d_eta4[e] * ex * u;
-                        Qc += ex * v;
                     }
                     double Af = 2.0 * f1 * f2 * f3;
                     double T1 = 2.0 * df1 * f2 * f3 * Q - 2.0 * r1 * Af * Qe;
@@ -821,24 +877,53 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
                     double Tc = Af * Qc;
                     double a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
                     double a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
-                    double g1x = a11 * d1.x + a12 * d2.x - a3 * wx, g1y = a11 * d1.y + a12 * d2.y - a3 * wy,
-                           g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
-                    double g2x = a22 * d2.x + a12 * d1.x + a3 * wx, g2y = a22 * d2.y + a12 * d1.y + a3 * wy,
-                           g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                    g1x = a11 * d1.x + a12 * d2.x - a3 * wx;
+                    g1y = a11 * d1.y + a12 * d2.y - a3 * wy;
+                    g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
+                    g2x = a22 * d2.x + a12 * d1.x + a3 * wx;
+                    g2y = a22 * d2.y + a12 * d1.y + a3 * wy;
+                    g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                    }
+                    }
                     fi[0] += g1x + g2x; fi[1] += g1y + g2y; fi[2] += g1z + g2z;
-                    atomicAdd(&s.Fnb[3 * jj], -g1x); atomicAdd(&s.Fnb[3 * jj + 1], -g1y); atomicAdd(&s.Fnb[3 * jj + 2], -g1z);
-                    atomicAdd(&s.Fnb[3 * kk], -g2x); atomicAdd(&s.Fnb[3 * kk + 1], -g2y); atomicAdd(&s.Fnb[3 * kk + 2], -g2z);
-                    vr[0] -= g1x * d1.x + g2x * d2.x;
-                    vr[1] -= g1y * d1.y + g2y * d2.y;
-                    vr[2] -= g1z * d1.z + g2z * d2.z;
-                    vr[3] -= g1x * d1.y + g2x * d2.y;
-                    vr[4] -= g1y * d1.z + g2y * d2.z;
-                    vr[5] -= g1z * d1.x + g2z * d2.x;
+                    if (on) {
+                        atomicAdd(&s.Fnb[3 * kk], -g2x);
+                        atomicAdd(&s.Fnb[3 * kk + 1], -g2y);
+                        atomicAdd(&s.Fnb[3 * kk + 2], -g2z);
+                    }
+                    /* j side: the list runs row by row, so lanes with the same j are
+                     * adjacent; sum each run and add it with one atomic */
+#pragma unroll
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const double ox = __shfl_down_sync(FULL, g1x, off), oy = __shfl_down_sync(FULL, g1y, off),
+                                     oz = __shfl_down_sync(FULL, g1z, off);
+                        const int ok = __shfl_down_sync(FULL, jj, off);
+                        if (lane + off < 32 && ok == jj) {
+                            g1x += ox;
+                            g1y += oy;
+                            g1z += oz;
+                        }
+                    }
+                    const int prev = __shfl_up_sync(FULL, jj, 1);
+                    if (valid && (lane == 0 || prev != jj)) {
+                        atomicAdd(&s.Fnb[3 * jj], -g1x);
+                        atomicAdd(&s.Fnb[3 * jj + 1], -g1y);
+                        atomicAdd(&s.Fnb[3 * jj + 2], -g1z);
+                    }
                 };
                 int *blk = s.blk + (blkid * WPA + warp) * 2;
-                for_block<WPA>(s, a, b, blk, reuse, tl_pos, tl_lo, tl_hi, warp, lane, accept_union, body);
+                for_block<WPA, true>(s, a, b, blk, reuse, tl_pos, tl_lo, tl_hi, warp, lane, accept_union, body);
                 group_sync<WPA>();
             }
+    }
+
+    /* virial of atom i's energy: every neighbour force (pairs and triplets)
+     * times its displacement -- the sum -(dE/dd) (x) d taken per neighbour */
+    for (int t = tid; t < n; t += NT) {
+        const double4 d = s.d[t];
+        const double fx = s.Fnb[3 * t], fy = s.Fnb[3 * t + 1], fz = s.Fnb[3 * t + 2];
+        vr[0] += fx * d.x; vr[1] += fy * d.y; vr[2] += fz * d.z;
+        vr[3] += fx * d.y; vr[4] += fy * d.z; vr[5] += fz * d.x;
     }
 
     /* ---- write forces and the virial of atom i ---- */
@@ -1184,5 +1269,83 @@ extern "C" int mbk_shape_ready(const mb_dev *d, int N, int mode) {
     const int key = (mode << 28) | (bucket << 20) | (d->capNB & 0xfffff);
     for (k = 0; k < d->tune_n; k++)
         if (d->tune_key[k] == key) return 1;
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Replayed single-structure passes: the kernel nodes of a captured     */
+/* pass that take the cell (or pV) by value, and their update          */
+/* ------------------------------------------------------------------ */
+
+template <typename... A>
+constexpr int karity(void (*)(A...)) {
+    return (int)sizeof...(A);
+}
+
+struct CellArg {
+    const void *func;
+    int arity, index; /* index of the mb_cell argument; -1: the pV argument of k_finalize */
+};
+
+static const CellArg kCellArgs[] = {
+    {(const void *)k_wrap, karity(k_wrap), 2},
+    {(const void *)k_cell_bin, karity(k_cell_bin), 2},
+    {(const void *)k_nlist_cell, karity(k_nlist_cell), 4},
+    {(const void *)k_nlist_brute, karity(k_nlist_brute), 4},
+    {(const void *)k_finalize, karity(k_finalize), -1},
+};
+
+/* Find in `graph` the kernel nodes whose arguments depend on the cell or
+ * pV; stores up to `cap` of them (node, table row) and returns how many
+ * there are, or -1 on an error. */
+extern "C" int mbk_graph_cell_nodes(void *graph, void **nodes, int *rows, int cap) {
+    size_t n = 0;
+    if (cudaGraphGetNodes((cudaGraph_t)graph, nullptr, &n) != cudaSuccess) return -1;
+    cudaGraphNode_t *all = (cudaGraphNode_t *)malloc(sizeof(cudaGraphNode_t) * (n ? n : 1));
+    if (cudaGraphGetNodes((cudaGraph_t)graph, all, &n) != cudaSuccess) {
+        free(all);
+        return -1;
+    }
+    int found = 0;
+    for (size_t k = 0; k < n; k++) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(all[k], &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        if (cudaGraphKernelNodeGetParams(all[k], &kp) != cudaSuccess) continue;
+        for (int r = 0; r < (int)(sizeof(kCellArgs) / sizeof(kCellArgs[0])); r++)
+            if (kp.func == kCellArgs[r].func) {
+                if (found < cap) {
+                    nodes[found] = (void *)all[k];
+                    rows[found] = r;
+                }
+                found++;
+            }
+    }
+    free(all);
+    return found;
+}
+
+/* Point the recorded nodes of the instantiated graph at a new cell and pV. */
+extern "C" int mbk_graph_set_cell(void *exec, void *const *nodes, const int *rows, int count, const mb_cell *c,
+                                  double pV) {
+    for (int k = 0; k < count; k++) {
+        cudaKernelNodeParams kp;
+        cudaError_t e = cudaGraphKernelNodeGetParams((cudaGraphNode_t)nodes[k], &kp);
+        if (e != cudaSuccess) return (int)e;
+        const CellArg &a = kCellArgs[rows[k]];
+        void *args[16];
+        if (a.arity > 16) return (int)cudaErrorInvalidValue;
+        for (int q = 0; q < a.arity; q++) args[q] = kp.kernelParams[q];
+        mb_cell cell = *c;
+        double pv = pV;
+        if (a.index >= 0)
+            args[a.index] = &cell;
+        else
+            args[2] = &pv;
+        kp.kernelParams = args;
+        kp.extra = nullptr;
+        e = cudaGraphExecKernelNodeSetParams((cudaGraphExec_t)exec, (cudaGraphNode_t)nodes[k], &kp);
+        if (e != cudaSuccess) return (int)e;
+    }
     return 0;
 }

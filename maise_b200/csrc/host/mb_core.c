@@ -33,6 +33,27 @@ typedef struct {
     size_t flush_bytes;
 } md_key;
 
+/* what a single-structure pass graph was captured for */
+typedef struct {
+    long gen;
+    int N, NM, ND, mode, M[3];
+    double urep;
+    void *h_res;
+} pass_key;
+
+#define MB_PASS_NODES 8
+
+typedef struct {
+    cudaGraph_t g;
+    cudaGraphExec_t x;
+    pass_key k;
+    void *nodes[MB_PASS_NODES];
+    int rows[MB_PASS_NODES], count;
+    long launches;
+    mb_cell last_c;
+    double last_pv;
+} pass_graph;
+
 struct mb_potential {
     mb_model m;
     int device;
@@ -53,6 +74,14 @@ struct mb_potential {
     md_key md_k;
     long md_launches;
     int md_st_events, md_ev_events;
+    /* single-structure pass graphs, one per mode (a relax alternates energy
+     * and energy+force passes): cell-dependent kernel nodes are re-pointed
+     * at each call's cell; results staged in pinned h_res */
+    pass_graph pgs[4];
+    int pbroken;
+    double *h_res; /* F[3N] then X[3N] of the last graphed pass */
+    size_t h_res_len;
+    int res_staged;
     /* timings moved out of the event pools (graph replays reuse the events) */
     double st_acc_ms, ev_acc_ms;
     int st_acc_n, ev_acc_n;
@@ -145,6 +174,14 @@ int mb_close(mb_potential *p) {
     cudaSetDevice(p->device);
     cudaStreamSynchronize(p->stream);
     if (p->md_exec) cudaGraphExecDestroy(p->md_exec);
+    {
+        int k;
+        for (k = 0; k < 4; k++) {
+            if (p->pgs[k].x) cudaGraphExecDestroy(p->pgs[k].x);
+            if (p->pgs[k].g) cudaGraphDestroy(p->pgs[k].g);
+        }
+    }
+    cudaFreeHost(p->h_res);
     dev_free(&p->d);
     cudaFree(p->d.params);
     cudaFree(p->d.weights);
@@ -469,6 +506,111 @@ static int upload(mb_potential *p, int N, int XT, const int *atmn, const double 
  * grow: the positions were already wrapped in place, so the caller
  * re-uploads them and calls again. */
 #define MB_RETRY 1000
+/* the device part of one pass, queued on the handle's stream: wrap, list,
+ * descriptor pass, finalize, then the status word and E, H, U to the host
+ * (and, with stage set, F and the wrapped X into the pinned h_res) */
+static int enqueue_pass(mb_potential *p, int N, int NM, const mb_cell *c, double pV, int mode, double urep,
+                        int stage) {
+    int r;
+    CK(cudaMemsetAsync(p->d.status, 0, sizeof(int) * 4, p->stream), "memset status");
+    if ((r = mbk_wrap(&p->d, N, c, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "wrap");
+    if ((r = mbk_nlist(&p->d, N, NM, c, p->m.rc_list, p->stream, &p->launches)))
+        return cuda_fail((cudaError_t)r, "neighbour list");
+    if ((r = mbk_descriptor_pass(&p->d, &p->m, N, mode, urep, 0, 0, p->stream, &p->launches)))
+        return cuda_fail((cudaError_t)r, "descriptor kernel");
+    if (mode != MB_MODE_DESCRIPTORS)
+        if ((r = mbk_finalize(&p->d, N, mode, pV, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "finalize");
+    CK(cudaMemcpyAsync(p->h_status, p->d.status, sizeof(int) * 4, cudaMemcpyDeviceToHost, p->stream), "D2H status");
+    CK(cudaMemcpyAsync(p->h_out, p->d.out, sizeof(double) * 16, cudaMemcpyDeviceToHost, p->stream), "D2H out");
+    if (stage) {
+        if (mode == MB_MODE_EFS || mode == MB_MODE_VJP)
+            CK(cudaMemcpyAsync(p->h_res, p->d.F, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, p->stream), "D2H F");
+        CK(cudaMemcpyAsync(p->h_res + 3 * N, p->d.X, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, p->stream),
+           "D2H X");
+    }
+    return MB_OK;
+}
+
+static void drop_pass_graph(pass_graph *q) {
+    if (q->x) cudaGraphExecDestroy(q->x);
+    if (q->g) cudaGraphDestroy(q->g);
+    q->x = NULL;
+    q->g = NULL;
+}
+
+/* Queue one pass as a replay of the captured pass graph of its mode,
+ * capturing it first if nothing matches (MB_FALLBACK when a graph cannot be
+ * used).  Between replays only the cell and pV change: the kernel nodes
+ * that take them by value are re-pointed at the new values. */
+#define MB_FALLBACK 1001
+static int graph_pass(mb_potential *p, int N, int NM, int ND, const mb_cell *c, double pV, int mode, double urep) {
+    pass_key k;
+    pass_graph *q = &p->pgs[mode & 3];
+    int r, m;
+    if (6 * (size_t)N > p->h_res_len) {
+        for (m = 0; m < 4; m++) drop_pass_graph(&p->pgs[m]);
+        cudaFreeHost(p->h_res);
+        p->h_res = NULL;
+        p->h_res_len = 0;
+        CK(cudaMallocHost((void **)&p->h_res, sizeof(double) * 6 * N), "cudaMallocHost");
+        p->h_res_len = 6 * (size_t)N;
+    }
+    memset(&k, 0, sizeof(k));
+    k.gen = p->gen;
+    k.N = N;
+    k.NM = NM;
+    k.ND = ND;
+    k.mode = mode;
+    k.M[0] = c->M[0];
+    k.M[1] = c->M[1];
+    k.M[2] = c->M[2];
+    k.urep = urep;
+    k.h_res = p->h_res;
+    if (!q->x || memcmp(&k, &q->k, sizeof(k))) {
+        cudaGraph_t g = NULL;
+        cudaError_t e;
+        const long l0 = p->launches;
+        const int expect = (ND > 0) + (c->M[0] > 0 ? 2 : 1) + (mode != MB_MODE_DESCRIPTORS);
+        drop_pass_graph(q);
+        CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        r = enqueue_pass(p, N, NM, c, pV, mode, urep, 1);
+        e = cudaStreamEndCapture(p->stream, &g);
+        if (r) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "end capture");
+        q->launches = p->launches - l0;
+        p->launches = l0;
+        q->count = mbk_graph_cell_nodes(g, q->nodes, q->rows, MB_PASS_NODES);
+        if (q->count != expect) {
+            /* the cell-dependent nodes were not all recognised: use plain launches */
+            cudaGraphDestroy(g);
+            p->pbroken = 1;
+            return MB_FALLBACK;
+        }
+        e = cudaGraphInstantiate(&q->x, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            q->x = NULL;
+            return cuda_fail(e, "graph instantiate");
+        }
+        q->g = g;
+        q->k = k;
+        q->last_c = *c;
+        q->last_pv = pV;
+    } else if (memcmp(c, &q->last_c, sizeof(*c)) || pV != q->last_pv) {
+        if ((r = mbk_graph_set_cell(q->x, q->nodes, q->rows, q->count, c, pV)))
+            return cuda_fail((cudaError_t)r, "graph node update");
+        q->last_c = *c;
+        q->last_pv = pV;
+    }
+    CK(cudaGraphLaunch(q->x, p->stream), "graph launch");
+    p->launches += q->launches;
+    p->res_staged = 1;
+    return MB_OK;
+}
+
 static int run_pass(mb_potential *p, int N, int NM, int ND, const double *lat9, int mode, double urep, double p_gpa) {
     mb_cell c;
     double pV = 0.0;
@@ -477,16 +619,13 @@ static int run_pass(mb_potential *p, int N, int NM, int ND, const double *lat9, 
     if (ND == 3) pV = p_gpa / MB_EV2GPA * cell_volume(lat9);
     ncell = c.M[0] ? c.M[0] * c.M[1] * c.M[2] : 1;
     if ((r = ensure(p, N, p->d.capNB ? p->d.capNB : (NM < 64 ? NM : 64), ncell))) return r;
-    CK(cudaMemsetAsync(p->d.status, 0, sizeof(int) * 4, p->stream), "memset status");
-    if ((r = mbk_wrap(&p->d, N, &c, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "wrap");
-    if ((r = mbk_nlist(&p->d, N, NM, &c, p->m.rc_list, p->stream, &p->launches)))
-        return cuda_fail((cudaError_t)r, "neighbour list");
-    if ((r = mbk_descriptor_pass(&p->d, &p->m, N, mode, urep, 0, 0, p->stream, &p->launches)))
-        return cuda_fail((cudaError_t)r, "descriptor kernel");
-    if (mode != MB_MODE_DESCRIPTORS)
-        if ((r = mbk_finalize(&p->d, N, mode, pV, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "finalize");
-    CK(cudaMemcpyAsync(p->h_status, p->d.status, sizeof(int) * 4, cudaMemcpyDeviceToHost, p->stream), "D2H status");
-    CK(cudaMemcpyAsync(p->h_out, p->d.out, sizeof(double) * 16, cudaMemcpyDeviceToHost, p->stream), "D2H out");
+    p->res_staged = 0;
+    r = MB_FALLBACK;
+    if (p->use_graphs && !p->pbroken && !p->d.ev_on && mbk_shape_ready(&p->d, N, mode)) {
+        r = graph_pass(p, N, NM, ND, &c, pV, mode, urep);
+        if (r != MB_OK && r != MB_FALLBACK) return r;
+    }
+    if (r == MB_FALLBACK && (r = enqueue_pass(p, N, NM, &c, pV, mode, urep, 0))) return r;
     CK(cudaStreamSynchronize(p->stream), "synchronize");
     if (p->h_status[0] & MB_ST_WRAP) return fail(MB_ERR_STATE, "non-finite or runaway positions");
     if (p->h_status[0] & MB_ST_NBR_OVERFLOW)
@@ -522,9 +661,17 @@ int mb_efs(mb_potential *p, int N, int NM, int ND, int XT, const int *atmn, cons
     if (E) *E = p->h_out[0];
     if (str)
         for (k = 0; k < 6; k++) str[k] = p->h_out[2 + k];
-    if (frc) CK(cudaMemcpyAsync(frc, p->d.F, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, p->stream), "D2H forces");
+    if (p->res_staged) {
+        /* the replayed pass left F and the wrapped X in pinned staging */
+        if (frc) memcpy(frc, p->h_res, sizeof(double) * 3 * N);
+        if (x_wrapped) memcpy(x_wrapped, p->h_res + 3 * N, sizeof(double) * 3 * N);
+        if (!ea) return MB_OK;
+    } else {
+        if (frc) CK(cudaMemcpyAsync(frc, p->d.F, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, p->stream), "D2H forces");
+        if (x_wrapped)
+            CK(cudaMemcpyAsync(x_wrapped, p->d.X, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, p->stream), "D2H X");
+    }
     if (ea) CK(cudaMemcpyAsync(ea, p->d.EA, sizeof(double) * N, cudaMemcpyDeviceToHost, p->stream), "D2H EA");
-    if (x_wrapped) CK(cudaMemcpyAsync(x_wrapped, p->d.X, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, p->stream), "D2H X");
     CK(cudaStreamSynchronize(p->stream), "synchronize");
     return MB_OK;
 }
@@ -638,7 +785,9 @@ static double relax_eval(relax_ctx *r, double *x, double *g) {
     if (!g) {
         rc = mb_energy(r->p, r->N, r->NM, r->ND, 1, r->atmn, r->L, r->xc, r->p_gpa, r->urep, &r->H, NULL, NULL);
         r->ne++;
-        if (!rc && cudaMemcpy(r->xc, r->p->d.X, sizeof(double) * 3 * r->N, cudaMemcpyDeviceToHost) != cudaSuccess)
+        if (!rc && r->p->res_staged)
+            memcpy(r->xc, r->p->h_res + 3 * r->N, sizeof(double) * 3 * r->N);
+        else if (!rc && cudaMemcpy(r->xc, r->p->d.X, sizeof(double) * 3 * r->N, cudaMemcpyDeviceToHost) != cudaSuccess)
             rc = fail(MB_ERR_CUDA, "D2H positions");
         if (rc) { r->err = rc; return NAN; }
     } else {

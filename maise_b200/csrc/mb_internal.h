@@ -144,6 +144,8 @@ int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, d
 int mbk_set_out(mb_dev *d, int idx, double v, void *stream);
 void mbk_record(void *event, void *stream);
 int mbk_shape_ready(const mb_dev *d, int N, int mode);
+int mbk_graph_cell_nodes(void *graph, void **nodes, int *rows, int cap);
+int mbk_graph_set_cell(void *exec, void *const *nodes, const int *rows, int count, const mb_cell *c, double pV);
 size_t mbk_efs_smem(const mb_model *m, int capNB, int shape);
 
 #ifdef __cplusplus

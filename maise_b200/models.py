@@ -133,13 +133,15 @@ def write_model(path, spcz, arch, nets, rmin, rmax, basis_text, model_id="B200RA
         f.write("\n".join(out) + "\n" + basis_text)
 
 
-def random_nets(nspc, arch, seed, binding=None):
+def random_nets(nspc, arch, seed, binding=None, angular=0.3):
     """N(0, 1/fan_in) networks.  With binding = (ind2 offsets, ng2) the G2
     inputs get positive first-layer weights, the second layer is positive and
     the output weights negative: the atomic energy then falls monotonically
     and saturates with coordination (an embedding-like binding), so that
     together with the short-range repulsion every structure has minima to
-    relax into.  G4 inputs keep small random weights."""
+    relax into.  G4 inputs keep random weights scaled by `angular` (larger
+    values make the energy depend more on the bond angles, so that structures
+    of one composition spread more in relaxed energy)."""
     D, h1, h2 = arch
     rng = np.random.default_rng(seed)
     nets = []
@@ -149,7 +151,7 @@ def random_nets(nspc, arch, seed, binding=None):
         W2 = rng.normal(0, 1 / np.sqrt(h2), h2)
         if binding is not None:
             offs, ng2 = binding
-            W0 *= 0.3
+            W0 *= angular
             for o in offs:
                 W0[:, o:o + ng2] = np.abs(rng.normal(0, 2.0 / np.sqrt(len(offs) * ng2), (h1, ng2)))
             W1 = np.abs(W1)
@@ -226,7 +228,8 @@ def sample_ranges(basis: Basis, X, LAT, atmn, ND, nspc, atoms_per_species=6, see
     return lo - 0.25 * span, hi + 0.25 * span
 
 
-def random_model(path, spcz, basis: Basis, sample, h=(10, 10), seed=1, model_id="B200RAND", binding=False):
+def random_model(path, spcz, basis: Basis, sample, h=(10, 10), seed=1, model_id="B200RAND", binding=False,
+                 angular=0.3):
     """Random-initialised model whose input ranges come from `sample` =
     (X, LAT, atmn, ND).  binding=True gives the sign structure of
     random_nets(binding=...) (used for relaxation workloads)."""
@@ -235,6 +238,6 @@ def random_model(path, spcz, basis: Basis, sample, h=(10, 10), seed=1, model_id=
     X, LAT, atmn, ND = sample
     lo, hi = sample_ranges(basis, X, LAT, atmn, ND, nspc, seed=seed)
     offs = [v * basis.ng2 + (v * (v + 1) // 2) * basis.ng4 for v in range(nspc)]
-    nets = random_nets(nspc, (D, h[0], h[1]), seed, binding=(offs, basis.ng2) if binding else None)
+    nets = random_nets(nspc, (D, h[0], h[1]), seed, binding=(offs, basis.ng2) if binding else None, angular=angular)
     write_model(path, spcz, (D, h[0], h[1]), nets, lo, hi, basis.text(), model_id=model_id)
     return path

@@ -274,3 +274,34 @@ def test_full_size_ternary_invariants(mb, tmp_path):
         Ep = pot.energy(Xp, w["LAT"], w["atmn"], ND=3, NM=200)["E"]
         Em = pot.energy(Xm, w["LAT"], w["atmn"], ND=3, NM=200)["E"]
         assert -(Ep - Em) / (2 * h) == pytest.approx(r["F"][i, q], abs=1e-6)
+
+
+@pytest.mark.parametrize("n", [2, 5])
+def test_replayed_pass_follows_cell_changes(mb, tmp_path, n):
+    """Single-structure passes replayed from a captured graph, with the cell
+    (and so the wrap, list and pV arguments) changing between calls as in a
+    cell relaxation, equal plain launches; 32 atoms use the all-pairs list,
+    500 the cell list."""
+    from maise_b200 import workloads
+
+    w = workloads.random_alloy(n=n, a=3.8, seed=12, species=(29, 46), jitter=0.06)
+    d = _model_for(tmp_path, w)
+    out = []
+    for graphs in (False, True):
+        pot = mb.Potential(d + "/model")
+        pot.graphs(graphs)
+        res = []
+        for k in range(6):
+            eps = np.array([[0.01 * k, 0.004 * k, 0.0], [0.0, -0.006 * k, 0.003 * k], [0.002 * k, 0.0, 0.008 * k]])
+            lat = w["LAT"] @ (np.eye(3) + eps)
+            r = pot.efs(w["X"] @ (np.eye(3) + eps), lat, w["atmn"], ND=3, NM=200, p_gpa=3.0 * k, urep=1.0)
+            e = pot.energy(w["X"] @ (np.eye(3) + eps), lat, w["atmn"], ND=3, NM=200)
+            res.append((r, e))
+        out.append(res)
+        pot.close()
+    for (r0, e0), (r1, e1) in zip(*out):
+        assert r1["H"] == pytest.approx(r0["H"], rel=1e-12)
+        assert e1["H"] == pytest.approx(e0["H"], rel=1e-12)
+        np.testing.assert_allclose(r1["F"], r0["F"], rtol=1e-10, atol=1e-12)
+        np.testing.assert_allclose(r1["U"], r0["U"], rtol=1e-10, atol=1e-10)
+        np.testing.assert_array_equal(r1["X"], r0["X"])

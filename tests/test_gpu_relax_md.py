@@ -148,3 +148,24 @@ def test_md_graph_replay_equals_plain_launches(mb, tmp_path, size):
         np.testing.assert_allclose(r1["H"], r0["H"], rtol=1e-11, atol=1e-9 * N)
         assert r1["xi"] == pytest.approx(r0["xi"], rel=1e-9, abs=1e-12)
     assert n1 == n0  # the replays count the launches they contain
+
+
+def test_relax_with_replayed_passes_equals_plain_launches(mb, tmp_path):
+    """A cell relaxation whose evaluations replay the captured pass graphs
+    (energy and energy+force passes alternate; the cell is re-pointed at each
+    call) follows the plain-launch path."""
+    from maise_b200 import models, workloads
+
+    rng = np.random.default_rng(21)
+    X, L, at = workloads.random_cell(10, rng, 2)
+    d = tmp_path / "m"
+    d.mkdir()
+    models.random_model(str(d / "model"), [12, 20], models.Basis(), (X, L, at, 3), seed=4)
+    res = []
+    for graphs in (False, True):
+        pot = mb.Potential(str(d / "model"))
+        pot.graphs(graphs)
+        res.append(pot.relax(X, L, at, ND=3, NM=300, rlxt=3, mitr=20, etol=1e-7, urep=100.0))
+        pot.close()
+    assert res[1]["H"] == pytest.approx(res[0]["H"], abs=1e-8)
+    np.testing.assert_allclose(res[1]["LAT"], res[0]["LAT"], atol=1e-8)

@@ -245,30 +245,43 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
     const BParams &P = *A.P;
     const int lane = threadIdx.x & 31;
     const int n = sh.nn[i], s0 = sh.spc[i], ns = P.nspc, D = P.D, ng2 = P.ng2;
-    /* stage neighbours sorted by relative species */
-    for (int t = lane; t < n; t += 32) ws.raw[t] = sh.spc[nbj[i * BMAXNB + t]];
-    __syncwarp();
-    if (lane == 0) {
-        int cnt[4] = {0, 0, 0, 0};
-        for (int t = 0; t < n; t++) cnt[(ws.raw[t] - s0 + ns) % ns]++;
-        int o = 0;
-        for (int v = 0; v < 4; v++) {
-            ws.seg[v] = cnt[v];
-            ws.seg[4 + v] = o;
-            o += cnt[v];
-        }
+    /* stage neighbours stably sorted by relative species: counts and ranks
+     * from warp ballots, one round per 32 neighbours */
+    int cnt[4] = {0, 0, 0, 0};
+    for (int base = 0; base < n; base += 32) {
+        const int t = base + lane;
+        const int ds = t < n ? (sh.spc[nbj[i * BMAXNB + t]] - s0 + ns) % ns : -1;
+#pragma unroll
+        for (int v = 0; v < 4; v++) cnt[v] += __popc(__ballot_sync(FULLM, ds == v));
     }
     for (int t = lane; t < D; t += 32) ws.G[t] = 0.0f;
+    if (lane < 4) {
+        int o = 0;
+        for (int v = 0; v < lane; v++) o += cnt[v];
+        ws.seg[lane] = cnt[lane];
+        ws.seg[4 + lane] = o;
+    }
     __syncwarp();
-    for (int t = lane; t < n; t += 32) {
-        int ds = (ws.raw[t] - s0 + ns) % ns, rank = 0;
-        for (int u = 0; u < t; u++) rank += ((ws.raw[u] - s0 + ns) % ns) == ds;
-        int dst = ws.seg[4 + ds] + rank;
-        float4 dv = nbd[i * BMAXNB + t];
-        ws.d[dst] = dv;
-        ws.ir[dst] = 1.0f / dv.w;
-        ws.j[dst] = nbj[i * BMAXNB + t];
-        ws.sp[dst] = ws.raw[t];
+    int run[4] = {0, 0, 0, 0};
+    const unsigned below = (1u << lane) - 1u;
+    for (int base = 0; base < n; base += 32) {
+        const int t = base + lane;
+        const int sp = t < n ? sh.spc[nbj[i * BMAXNB + t]] : 0;
+        const int ds = t < n ? (sp - s0 + ns) % ns : -1;
+        int dst = 0;
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const unsigned m = __ballot_sync(FULLM, ds == v);
+            if (ds == v) dst = ws.seg[4 + v] + run[v] + __popc(m & below);
+            run[v] += __popc(m);
+        }
+        if (t < n) {
+            const float4 dv = nbd[i * BMAXNB + t];
+            ws.d[dst] = dv;
+            ws.ir[dst] = 1.0f / dv.w;
+            ws.j[dst] = nbj[i * BMAXNB + t];
+            ws.sp[dst] = sp;
+        }
     }
     __syncwarp();
 
@@ -324,7 +337,7 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
 #pragma unroll
             for (int k = 0; k < BCELLS; k++) acc[k] = 0.0f;
             const int na = ws.seg[a], nb = ws.seg[b], oa = ws.seg[4 + a], ob = ws.seg[4 + b];
-            int row = 0, start = tl_pos;
+            int start = tl_pos;
             /* j and k species are fixed within the block: hoist their parameters */
             const int sja = (a + s0) % ns, skb = (b + s0) % ns;
             const int p01 = s0 * s0 + sja * sja, p02 = s0 * s0 + skb * skb, p12 = sja * sja + skb * skb;
@@ -334,25 +347,33 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
             float eta12[BNE];
 #pragma unroll
             for (int e = 0; e < BNE; e++) eta12[e] = P.f_eta4[p12][e];
+            /* candidates (row, col) of the block in row-major order, 32 per
+             * round with every lane busy: row = (c + 0.5) / nb in FP32 is exact
+             * (the fraction stays >= 0.5 / nb from an integer) */
+            const int C = na * nb;
+            const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f;
+            int c = 0;
             for (;;) {
                 int from = tl_pos;
-                for (; row < na; row++) {
-                    int jj = oa + row, k0 = (a == b) ? row + 1 : 0;
-                    if (tl_pos + (nb - k0) > BTL) break;
-                    for (int kb = k0; kb < nb; kb += 32) {
-                        int kk = ob + kb + lane;
-                        bool ok = false;
-                        if (kb + lane < nb) {
+                for (; c < C && tl_pos + 32 <= BTL; c += 32) {
+                    const int cc = c + lane;
+                    bool ok = false;
+                    int jj = 0, kk = 0;
+                    if (cc < C) {
+                        const int r = __float2int_rz(((float)cc + 0.5f) * inv_nb), col = cc - r * nb;
+                        jj = oa + r;
+                        kk = ob + col;
+                        if (a != b || col > r) {
                             const float4 d1 = ws.d[jj], d2 = ws.d[kk];
                             const float dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
                             const float r3s = dx * dx + dy * dy + dz * dz;
                             ok = (d1.w < rc2_01 && d1.w < rc4_01 && d2.w < rc4_02 && r3s < rc4sq_12) ||
                                  (d1.w < drc4 && d2.w < drc4 && r3s < drc4sq);
                         }
-                        unsigned m = __ballot_sync(FULLM, ok);
-                        if (ok) ws.tl[tl_pos + __popc(m & ((1u << lane) - 1u))] = (unsigned)jj | ((unsigned)kk << 16);
-                        tl_pos += __popc(m);
                     }
+                    const unsigned m = __ballot_sync(FULLM, ok);
+                    if (ok) ws.tl[tl_pos + __popc(m & ((1u << lane) - 1u))] = (unsigned)jj | ((unsigned)kk << 16);
+                    tl_pos += __popc(m);
                 }
                 __syncwarp();
                 for (int t = from + lane; t < tl_pos; t += 32) {
@@ -373,13 +394,20 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
                                           jb.x * kb4.x, jb.y * kb4.y, jb.z * kb4.z, jb.w * kb4.w};
 #pragma unroll
                     for (int e = 0; e < BNE; e++) {
-                        float ex = A3 * pjk[e] * expf(-eta12[e] * r3s);
+                        const float ex = A3 * pjk[e] * expf(-eta12[e] * r3s);
+                        const float2 ex2 = make_float2(ex, ex);
+                        /* paired FP32 FMAs: two grid cells per instruction */
 #pragma unroll
-                        for (int zl = 0; zl < BNZL; zl++) acc[e * BNZL + zl] += ex * lz[zl];
+                        for (int zl = 0; zl < BNZL; zl += 2) {
+                            const float2 r = __ffma2_rn(ex2, make_float2(lz[zl], lz[zl + 1]),
+                                                        make_float2(acc[e * BNZL + zl], acc[e * BNZL + zl + 1]));
+                            acc[e * BNZL + zl] = r.x;
+                            acc[e * BNZL + zl + 1] = r.y;
+                        }
                     }
                 }
                 __syncwarp();
-                if (row >= na) break;
+                if (c >= C) break;
                 whole = 0;
                 start = tl_pos = 0;
             }
@@ -390,9 +418,9 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
             ws.red[2 * lane] = acc[0];
             ws.red[2 * lane + 1] = acc[1];
             __syncwarp();
-            if (lane == 0) {
-                int base = P.ind4[a * a + b * b];
-                for (int f = 0; f < P.ng4; f++) ws.G[base + f] += ws.red[P.g4_cell[f]];
+            {
+                const int base = P.ind4[a * a + b * b];
+                for (int f = lane; f < P.ng4; f += 32) ws.G[base + f] += ws.red[P.g4_cell[f]];
             }
             __syncwarp();
         }
@@ -484,8 +512,7 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
             const int base = P.ind4[a * a + b * b];
             for (int t = lane; t < BCELLS; t += 32) ws.grid[t] = 0.0f;
             __syncwarp();
-            if (lane == 0)
-                for (int f = 0; f < P.ng4; f++) ws.grid[P.g4_cell[f]] += ws.G[base + f];
+            for (int f = lane; f < P.ng4; f += 32) atomicAdd(&ws.grid[P.g4_cell[f]], ws.G[base + f]);
             __syncwarp();
             const int na = ws.seg[a], nb = ws.seg[b], oa = ws.seg[4 + a], ob = ws.seg[4 + b];
             int row = 0, lo = whole ? ws.blk[blkid][0] : 0, hi = whole ? ws.blk[blkid][1] : 0;
@@ -542,12 +569,12 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
                         const float ex = pjk[q] * expf(-deta[q] * r3s);
                         const float4 ga = g4[2 * q], gb = g4[2 * q + 1];
                         const float cg[8] = {ga.x, ga.y, ga.z, ga.w, gb.x, gb.y, gb.z, gb.w};
-                        float u = 0.0f, vv = 0.0f;
+                        /* (u, v) = sum over cells of cg * (lz, lz') with paired FMAs */
+                        float2 uv = make_float2(0.0f, 0.0f);
 #pragma unroll
-                        for (int zl = 0; zl < BNZL; zl++) {
-                            u += cg[zl] * lz[zl];
-                            vv += cg[zl] * lzp[zl];
-                        }
+                        for (int zl = 0; zl < BNZL; zl++)
+                            uv = __ffma2_rn(make_float2(cg[zl], cg[zl]), make_float2(lz[zl], lzp[zl]), uv);
+                        const float u = uv.x, vv = uv.y;
                         Q += ex * u;
                         Qe += deta[q] * ex * u;
                         Qc += ex * vv;
@@ -742,7 +769,14 @@ __device__ double evaluate(const BArgs &A, BShared &sh, const double *dof, doubl
     /* FP64 reductions, enthalpy and the DOF gradient (cdfunc_gsl, src/cmin.c:107-166) */
     if (tid == 0) {
         double E = 0.0, U[6];
-        for (int a = 0; a < N; a++) E += sh.ea[a] + sh.eu[a];
+        double mag = 0.0;
+        for (int a = 0; a < N; a++) {
+            E += sh.ea[a] + sh.eu[a];
+            mag += fabs(sh.ea[a]);
+        }
+        /* rounding floor of the enthalpy: the per-atom energies come from FP32
+         * descriptors and MLP, a few ulps each */
+        sh.scal[3] = 4.0 * 1.1920929e-7 * mag;
         for (int k = 0; k < 6; k++) {
             U[k] = 0.0;
             for (int ww = 0; ww < BWARPS; ww++) U[k] += sh.vir[ww][k];
@@ -899,6 +933,9 @@ __global__ void __launch_bounds__(BWARPS * 32) k_relax_batch(BArgs A) {
             /* Fletcher line search with energy and gradient at every trial */
             double ap = 0.0, fp = f, dp = dphi0, a = 0, fa = 0, da = 0, b = 0, fb = 0, db = 0;
             double a_maxf = maxf, a_maxu = maxu, ft = 0.0, dt;
+            /* energy comparisons allow the FP32 rounding floor: below it only
+             * the (accurate) directional derivative can tell progress */
+            const double epsE = sh.scal[3];
             int phase = 0, done = 0, trial;
             vcopy(sh.xa, sh.x, n);
             vcopy(sh.ga, sh.g, n);
@@ -916,7 +953,7 @@ __global__ void __launch_bounds__(BWARPS * 32) k_relax_batch(BArgs A) {
                 double next = alpha;
                 if (!isfinite(ft)) { done = 4; break; }
                 if (phase == 0) {
-                    if (ft > f + rho * alpha * dphi0 || (trial > 0 && ft >= fp)) {
+                    if (ft > f + rho * alpha * dphi0 + epsE || (trial > 0 && ft >= fp + epsE)) {
                         a = ap; fa = fp; da = dp; b = alpha; fb = ft; db = dt;
                         phase = 1;
                     } else if (fabs(dt) <= -A.sigma * dphi0) {
@@ -931,7 +968,7 @@ __global__ void __launch_bounds__(BWARPS * 32) k_relax_batch(BArgs A) {
                         save_a = 1;
                     }
                 } else {
-                    if (ft > f + rho * alpha * dphi0 || ft >= fa) {
+                    if (ft > f + rho * alpha * dphi0 + epsE || ft >= fa + epsE) {
                         b = alpha; fb = ft; db = dt;
                     } else if (fabs(dt) <= -A.sigma * dphi0) {
                         done = 1;
@@ -966,7 +1003,7 @@ __global__ void __launch_bounds__(BWARPS * 32) k_relax_batch(BArgs A) {
             if (done == 3) { status = 2; break; }
             if (done == 2 || done == 4 || done == 0) {
                 /* accept the best bracketed point if it lowered the enthalpy */
-                if (phase == 1 && a > 0.0 && fa < f) {
+                if (phase == 1 && a > 0.0 && fa < f + epsE) {
                     vcopy(sh.xt, sh.xa, n);
                     vcopy(sh.gt, sh.ga, n);
                     alpha = a;
@@ -974,6 +1011,13 @@ __global__ void __launch_bounds__(BWARPS * 32) k_relax_batch(BArgs A) {
                     maxf = a_maxf;
                     maxu = a_maxu;
                     __syncthreads();
+                } else if (!first) {
+                    /* no acceptable step along the quasi-Newton direction:
+                     * restart once from steepest descent before giving up */
+                    for (int k = tid; k < n * n; k += blockDim.x) H[k] = (k / n == k % n) ? 1.0 : 0.0;
+                    first = 1;
+                    __syncthreads();
+                    continue;
                 } else {
                     status = 3;
                     break;

@@ -376,9 +376,12 @@ __host__ __device__ inline size_t efs_smem_bytes(int cap, int D, int ne, int ng2
     b += align16(sizeof(double) * D);             /* G */
     b += sizeof(double) * nzl_cells;              /* grid */
     b += sizeof(double) * warps * 64;             /* red */
-    b += sizeof(double) * cap * (ng2 > 1 ? ng2 : 1); /* tmp */
+    /* tmp (G2 terms) and tl (triplet list) share one region: tmp is dead
+     * before the first list entry is written */
+    const size_t tmp_b = sizeof(double) * cap * (ng2 > 1 ? ng2 : 1), tl_b = align8(sizeof(unsigned) * tl);
+    b += tmp_b > tl_b ? tmp_b : tl_b; /* tmp | tl */
     b += sizeof(double) * 4 * MB_MAXH;            /* h */
-    b += align8(sizeof(unsigned) * tl);           /* tl */
+
     b += align8(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
     b += sizeof(int) * 8;
     return b;
@@ -397,12 +400,16 @@ __device__ inline EfsSmem efs_carve(char *base, int cap, int D, int ne, int ng2,
     s.G = (double *)p; p += align16(sizeof(double) * D);
     s.grid = (double *)p; p += sizeof(double) * nzl_cells;
     s.red = (double *)p; p += sizeof(double) * warps * 64;
-    s.tmp = (double *)p; p += sizeof(double) * cap * (ng2 > 1 ? ng2 : 1);
+    {
+        const size_t tmp_b = sizeof(double) * cap * (ng2 > 1 ? ng2 : 1), tl_b = align8(sizeof(unsigned) * tl);
+        s.tmp = (double *)p;
+        s.tl = (unsigned *)p;
+        p += tmp_b > tl_b ? tmp_b : tl_b;
+    }
     s.h = (double *)p; p += sizeof(double) * 4 * MB_MAXH;
     s.j = (int *)p; p += align8(sizeof(int) * cap);
     s.sp = (int *)p; p += align8(sizeof(int) * cap);
     s.raw_sp = (int *)p; p += align8(sizeof(int) * cap);
-    s.tl = (unsigned *)p; p += align8(sizeof(unsigned) * tl);
     s.blk = (int *)p; p += align8(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
     s.seg = (int *)p;
     return s;
@@ -470,23 +477,34 @@ __device__ __forceinline__ void group_reduce64(double *v, EfsSmem &s, int gwarp,
  * the group's warps; each warp appends its accepted pairs to its own region
  * [lo,hi) of the list, a row at a time, and stops before a row that might
  * not fit.  Returns the next unprocessed row of this warp. */
+/* Append the accepted candidates (j, k) of block (a, b) to this warp's
+ * list region: the block's (row, col) square in row-major order, 32
+ * candidates per round with every lane busy, the warps of an atom taking
+ * every WPA-th round (row = (c + 0.5) / nb in FP32 is exact: the fraction
+ * stays >= 0.5 / nb away from an integer).  Returns the next candidate
+ * index; stops early when the region is full. */
 template <int WPA, class Accept>
-__device__ __forceinline__ int fill_rows(const EfsSmem &s, int a, int b, int row, int &pos, int hi, int lane,
-                                         Accept accept) {
+__device__ __forceinline__ int fill_chunks(const EfsSmem &s, int a, int b, int c, int &pos, int hi, int lane,
+                                           Accept accept) {
     const int na = s.seg[a], nb = s.seg[b], oa = s.seg[4 + a], ob = s.seg[4 + b];
-    for (; row < na; row += WPA) {
-        const int jj = oa + row, k0 = (a == b) ? row + 1 : 0;
-        if (pos + (nb - k0) > hi) break;
-        for (int kb = k0; kb < nb; kb += 32) {
-            const int kk = ob + kb + lane;
-            const bool ok = (kb + lane < nb) && accept(jj, kk);
-            const unsigned m = __ballot_sync(FULL, ok);
-            if (ok) s.tl[pos + __popc(m & ((1u << lane) - 1u))] = (unsigned)jj | ((unsigned)kk << 16);
-            pos += __popc(m);
+    const int C = na * nb;
+    const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f;
+    for (; c < C && pos + 32 <= hi; c += 32 * WPA) {
+        const int cc = c + lane;
+        bool ok = false;
+        int jj = 0, kk = 0;
+        if (cc < C) {
+            const int r = __float2int_rz(((float)cc + 0.5f) * inv_nb), col = cc - r * nb;
+            jj = oa + r;
+            kk = ob + col;
+            ok = (a != b || col > r) && accept(jj, kk);
         }
+        const unsigned m = __ballot_sync(FULL, ok);
+        if (ok) s.tl[pos + __popc(m & ((1u << lane) - 1u))] = (unsigned)jj | ((unsigned)kk << 16);
+        pos += __popc(m);
     }
     __syncwarp();
-    return row;
+    return c;
 }
 
 /* body(jj, kk) over list entries [from, to), one entry per lane */
@@ -528,16 +546,17 @@ __device__ __forceinline__ int for_block(const EfsSmem &s, int a, int b, int *bl
             run_list(s, blk[0], blk[1], lane, body);
         return 1;
     }
-    int start = pos, row = warp, whole = 1;
+    int start = pos, c = warp * 32, whole = 1;
+    const int C = s.seg[a] * s.seg[b];
     for (;;) {
         const int from = pos;
-        row = fill_rows<WPA>(s, a, b, row, pos, hi, lane, accept);
+        c = fill_chunks<WPA>(s, a, b, c, pos, hi, lane, accept);
         if constexpr (ALL)
             run_list_all(s, from, pos, lane, body);
         else
             run_list(s, from, pos, lane, body);
         __syncwarp();
-        if (row >= s.seg[a]) break;
+        if (c >= C) break;
         whole = 0; /* region full: restart it for the next round */
         start = pos = lo;
     }
@@ -647,6 +666,7 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
         }
         A.EU[i] = eu;
     }
+    group_sync<WPA>(); /* the G2 terms in tmp are read; the triplet list reuses their space */
 
     /* ---- forward triplet terms, block by block of (species j, species k) ---- */
     {

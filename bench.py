@@ -119,6 +119,19 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(seconds, dist=None):
+    """The slowest rank's time: the job finishes when its last replica does.
+    Works over NCCL (CUDA tensor) or gloo (CPU tensor)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(seconds)
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -410,11 +423,7 @@ def main():
     pot.md_profile(False)
     pot.profile(False)
     clocks = sampler.stop()
-    step_s = steps_t["ms_total"] / 1e3
-    if dist is not None:
-        t = torch.tensor([step_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_s = float(t.item())
+    step_s = max_over_ranks(steps_t["ms_total"] / 1e3, dist)
     value = world * N * args.steps / step_s
 
     # end to end through the C-ABI: host positions in, host forces out, host NVT update
@@ -434,11 +443,7 @@ def main():
         Ve = Ve + f
     e1.record(stream)
     e1.synchronize()
-    e2e_s = e0.elapsed_time(e1) / 1e3
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
     e2e = {"value": world * N * k2 / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8 + N * 4 + 9 * 8,
            "d2h_bytes_per_step": 3 * N * 8 + N * 8 + 3 * N * 8 + 16 * 8}
 

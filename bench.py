@@ -361,6 +361,7 @@ def main():
                     help="run one small case of a hot kernel for an ncu capture and exit (no bench line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    t_start = time.perf_counter()
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -468,13 +469,20 @@ def main():
                        "l2": "256 MiB buffer overwritten between timed steps (outside the step events)",
                        "model": "random N(0,1/fan_in) weights, input ranges from the structure"},
             "e2e": e2e, "roofline": roof, "gpu_launches": launches, "clocks": clocks}
+    def leg(name, fn):
+        t0 = time.perf_counter()
+        r = fn()
+        print(f"[bench] {name}: {time.perf_counter() - t0:.1f} s", file=sys.stderr, flush=True)
+        return r
+
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w, td)
+        line["cpu_baseline"] = leg("cpu_baseline", lambda: cpu_baseline(w, td))
     if rank == 0 and not args.no_population:
-        line["population_relax"] = population_relax(local, td)
-        line["surrogate_generation"] = surrogate_generation(local, td)
+        line["population_relax"] = leg("population_relax", lambda: population_relax(local, td))
+        line["surrogate_generation"] = leg("surrogate_generation", lambda: surrogate_generation(local, td))
     if rank == 0:
         print(json.dumps(line))
+        print(f"[bench] total: {time.perf_counter() - t_start:.1f} s", file=sys.stderr, flush=True)
     pot.close()
     if dist is not None:
         dist.barrier()

@@ -52,6 +52,8 @@ typedef struct {
     long launches;
     mb_cell last_c;
     double last_pv;
+    pass_key seen; /* last key run without a graph: captured when it repeats */
+    int seen_valid;
 } pass_graph;
 
 struct mb_potential {
@@ -568,6 +570,13 @@ static int graph_pass(mb_potential *p, int N, int NM, int ND, const mb_cell *c, 
     k.h_res = p->h_res;
     if (!q->x || memcmp(&k, &q->k, sizeof(k))) {
         cudaGraph_t g = NULL;
+        if (!q->seen_valid || memcmp(&k, &q->seen, sizeof(k))) {
+            /* a key met once (e.g. a loop over structures of many sizes) is not
+             * worth a capture: run it plainly and capture if it comes again */
+            q->seen = k;
+            q->seen_valid = 1;
+            return MB_FALLBACK;
+        }
         cudaError_t e;
         const long l0 = p->launches;
         const int expect = (ND > 0) + (c->M[0] > 0 ? 2 : 1) + (mode != MB_MODE_DESCRIPTORS);

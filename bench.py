@@ -245,8 +245,8 @@ def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs
     from maise_b200.surrogate import Surrogate, keep_best, recall
 
     spc = (29, 46, 47)
-    train = workloads.ea_population(count=n_train, nmin=16, nmax=48, seed=11, species=spc)
-    gen = workloads.ea_population(count=n_gen, nmin=16, nmax=48, seed=12, species=spc)
+    train = workloads.ea_population_chunked(n_train, seed=11, nmin=16, nmax=48, species=spc)
+    gen = workloads.ea_population_chunked(n_gen, seed=12, nmin=16, nmax=48, species=spc)
     pot = maise_b200.Potential(_binding_model(td, "gen", train, spc, 5), device=local)
     t0 = time.perf_counter()
     rt = pot.relax_batch(train, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
@@ -301,7 +301,7 @@ def profile_case(case):
     else:
         from maise_b200.surrogate import Surrogate
 
-        pop = workloads.ea_population(count=512, nmin=16, nmax=48, seed=11, species=(29, 46, 47))
+        pop = workloads.ea_population_chunked(512, seed=11, nmin=16, nmax=48, species=(29, 46, 47))
         sur = Surrogate(3)
         feat = sur.features(pop)
         sur.fit(feat, np.linspace(-4.0, -3.0, len(pop)), epochs=5, batch=256)

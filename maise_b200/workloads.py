@@ -68,6 +68,43 @@ def _min_image_dist(L, xf_new, xf_old):
     return best
 
 
+_SHIFTS = np.array([[i, j, k] for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)], float)
+
+
+def _min_image_dist_batch(L, cands, xf_old):
+    """_min_image_dist for a batch of candidates at once: [B] minimum image
+    distances of cands[B, 3] (fractional) to the atoms xf_old[M, 3]."""
+    d = xf_old[None, :, :] - cands[:, None, :]
+    d -= np.round(d)
+    v = (d[:, :, None, :] + _SHIFTS[None, None, :, :]) @ L
+    return np.sqrt((v * v).sum(-1)).min(axis=(1, 2))
+
+
+def _place(rng, L, xf, dmin, tries=2000, batch=64):
+    """Next atom by rejection (uniform fractional candidates, minimum image
+    distance >= dmin), scoring candidates in batches of 2, 4, ... up to
+    `batch` (most atoms are accepted at the first candidate).  The random
+    stream is consumed exactly as by one candidate at a time: after a batch
+    the state is restored and only the candidates up to the accepted one are
+    re-drawn.  Returns the accepted position or None."""
+    if len(xf) == 0:
+        return rng.uniform(0, 1, 3)
+    done, size = 0, 2
+    while done < tries:
+        b = min(size, tries - done)
+        size = min(2 * size, batch)
+        saved = rng.bit_generator.state
+        cands = rng.uniform(0, 1, (b, 3))
+        ok = _min_image_dist_batch(L, cands, xf) >= dmin
+        if ok.any():
+            i = int(np.argmax(ok))
+            rng.bit_generator.state = saved
+            rng.uniform(0, 1, (i + 1, 3))
+            return cands[i]
+        done += b
+    return None
+
+
 def random_cell(N, rng, species_count, vol_per_atom=20.0, spread=0.15, dmin=2.0, max_tries=200, composition=None):
     """EA-style random structure (cf. RAND_CL, src/eutl.c:276-390).  Species
     are drawn at random unless `composition` gives integer ratios (N must be
@@ -86,14 +123,11 @@ def random_cell(N, rng, species_count, vol_per_atom=20.0, spread=0.15, dmin=2.0,
         xf = np.zeros((0, 3))
         ok = True
         for _k in range(N):
-            for _t in range(2000):
-                cand = rng.uniform(0, 1, 3)
-                if len(xf) == 0 or _min_image_dist(L, cand, xf) >= dmin:
-                    xf = np.vstack([xf, cand])
-                    break
-            else:
+            cand = _place(rng, L, xf, dmin)
+            if cand is None:
                 ok = False
                 break
+            xf = np.vstack([xf, cand])
         if not ok:
             continue
         if composition is None:
@@ -141,3 +175,27 @@ def fcc_particle(n_target=20000, a=4.08, vacancy=0.05, jitter=0.05, pad=15.0, se
     LAT = np.eye(3) * box
     atmn = np.zeros(len(X), np.int32)
     return dict(X=X, LAT=LAT, atmn=atmn, ND=0, spcz=list(species))
+
+
+def _population_chunk(args):
+    count, seed, k, kw = args
+    return ea_population(count=count, seed=[seed, k], **kw)
+
+
+def ea_population_chunked(count, seed=0, chunk=256, workers=None, **kw):
+    """ea_population in independent chunks: chunk k holds `chunk` structures
+    drawn from the generator seeded by (seed, k), so the population depends
+    on (count, seed, chunk) only, not on how many worker processes build it.
+    Workers are started with `spawn` (safe next to a CUDA context)."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    import os
+
+    jobs = [(min(chunk, count - k * chunk), seed, k, kw) for k in range((count + chunk - 1) // chunk)]
+    workers = workers or min(len(jobs), os.cpu_count() or 1)
+    if workers <= 1:
+        parts = [_population_chunk(j) for j in jobs]
+    else:
+        with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            parts = list(ex.map(_population_chunk, jobs))
+    return [s for part in parts for s in part]

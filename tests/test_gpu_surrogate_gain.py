@@ -25,8 +25,8 @@ def test_screen_recalls_best_offspring_better_than_baselines(tmp_path):
     from maise_b200 import models, workloads
     from maise_b200.surrogate import Surrogate, keep_best, recall
 
-    train = workloads.ea_population(count=2000, nmin=16, nmax=48, seed=31, species=SPC)
-    gen = workloads.ea_population(count=200, nmin=16, nmax=48, seed=32, species=SPC)
+    train = workloads.ea_population_chunked(2000, seed=31, nmin=16, nmax=48, species=SPC)
+    gen = workloads.ea_population_chunked(200, seed=32, nmin=16, nmax=48, species=SPC)
     big = max(train, key=lambda s: len(s["atmn"]))
     models.random_model(str(tmp_path / "model"), list(SPC), models.Basis(), (big["X"], big["LAT"], big["atmn"], 3),
                         seed=5, binding=True)

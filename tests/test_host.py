@@ -138,3 +138,33 @@ def test_workload_generators():
     w4 = workloads.fcc_particle(n_target=2000, seed=1)
     assert 1800 <= len(w4["atmn"]) <= 2200 and w4["ND"] == 0
     assert (w4["X"] > 14.0).all() and (w4["X"] < w4["LAT"][0, 0] - 14.0).all()
+
+
+def test_vectorised_cell_placement_keeps_the_random_stream():
+    """Batched candidate scoring consumes the generator exactly as one
+    candidate at a time, so a seed's population does not change."""
+    import numpy as np
+
+    from maise_b200 import workloads
+
+    L0 = np.diag([6.0, 6.5, 7.0])
+    rng_a, rng_b = np.random.default_rng(7), np.random.default_rng(7)
+    pa, pb = [], []
+    for _ in range(12):
+        pa.append(workloads._place(rng_a, L0, np.array(pa).reshape(-1, 3), 2.0, batch=64))
+        pb.append(workloads._place(rng_b, L0, np.array(pb).reshape(-1, 3), 2.0, batch=1))
+    np.testing.assert_array_equal(np.array(pa), np.array(pb))
+    assert rng_a.uniform() == rng_b.uniform()
+
+
+def test_chunked_population_does_not_depend_on_workers():
+    import numpy as np
+
+    from maise_b200 import workloads
+
+    a = workloads.ea_population_chunked(70, seed=4, chunk=32, workers=1, nmin=8, nmax=12)
+    b = workloads.ea_population_chunked(70, seed=4, chunk=32, workers=2, nmin=8, nmax=12)
+    assert len(a) == len(b) == 70
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x["X"], y["X"])
+        np.testing.assert_array_equal(x["atmn"], y["atmn"])

@@ -350,9 +350,10 @@ struct EfsArgs {
 
 /* shared-memory carve-up of one atom group of k_efs */
 struct EfsSmem {
-    int *j, *sp, *raw_sp;
+    int *j, *sp;
     double4 *d;
     double *ir, *fa, *fb, *P, *Fnb, *G, *grid, *red, *tmp, *h;
+    double *stage; /* per warp: 32 triplets x EFS_STG doubles (tensor-core forward) */
     unsigned *tl;  /* accepted (j,k) pairs: per-warp regions of tlw entries */
     int *blk;      /* [block][warp][2] ranges of each warp's region per species block */
     int *seg;      /* [0..3] counts, [4..7] offsets */
@@ -366,50 +367,61 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t
  * start on 16 bytes (the neighbour capacity is a multiple of 8) */
 __host__ __device__ constexpr int nep(int ne) { return (ne + 1) & ~1; }
 
-__host__ __device__ inline size_t efs_smem_bytes(int cap, int D, int ne, int ng2, int nzl_cells, int warps, int tl) {
+#define EFS_STG 17 /* staging row: 8 exponential + 8 angular values + 1 pad (banks) */
+
+/* Sizes of the regions that share one block of memory: the forward
+ * staging rows (tensor-core forward, live only while the forward triplets
+ * run) and Fnb + grid + red + h (block reductions, MLP and reverse pass,
+ * all after it). */
+__host__ __device__ inline size_t efs_union_bytes(int cap, int nzl_cells, int warps, int stage) {
+    const size_t st = stage ? sizeof(double) * warps * 32 * EFS_STG : 0;
+    const size_t rest = sizeof(double) * (cap * 3 + nzl_cells + warps * 64 + 4 * MB_MAXH);
+    return align16(st > rest ? st : rest);
+}
+
+__host__ __device__ inline size_t efs_smem_bytes(int cap, int D, int ne, int ng2, int nzl_cells, int warps, int tl,
+                                                 int stage) {
     size_t b = 0;
-    b += align8(sizeof(int) * cap) * 3;           /* j, sp, raw_sp */
+    b += efs_union_bytes(cap, nzl_cells, warps, stage); /* stage | Fnb, grid, red, h */
+    b += align8(sizeof(int) * cap) * 2;           /* j, sp */
     b += sizeof(double4) * cap;                   /* d */
     b += sizeof(double) * cap * 3;                /* ir, fa, fb */
     b += sizeof(double) * cap * nep(ne);          /* P */
-    b += sizeof(double) * cap * 3;                /* Fnb */
     b += align16(sizeof(double) * D);             /* G */
-    b += sizeof(double) * nzl_cells;              /* grid */
-    b += sizeof(double) * warps * 64;             /* red */
     /* tmp (G2 terms) and tl (triplet list) share one region: tmp is dead
      * before the first list entry is written */
     const size_t tmp_b = sizeof(double) * cap * (ng2 > 1 ? ng2 : 1), tl_b = align8(sizeof(unsigned) * tl);
     b += tmp_b > tl_b ? tmp_b : tl_b; /* tmp | tl */
-    b += sizeof(double) * 4 * MB_MAXH;            /* h */
-
     b += align8(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
     b += sizeof(int) * 8;
     return b;
 }
 
-__device__ inline EfsSmem efs_carve(char *base, int cap, int D, int ne, int ng2, int nzl_cells, int warps, int tl) {
+__device__ inline EfsSmem efs_carve(char *base, int cap, int D, int ne, int ng2, int nzl_cells, int warps, int tl,
+                                   int stage) {
     /* one atom group's region; `warps` = warps per atom */
     EfsSmem s;
     char *p = base;
+    s.stage = (double *)p;
+    s.Fnb = (double *)p;
+    s.grid = s.Fnb + cap * 3;
+    s.red = s.grid + nzl_cells;
+    s.h = s.red + warps * 64;
+    p += efs_union_bytes(cap, nzl_cells, warps, stage);
     s.d = (double4 *)p; p += sizeof(double4) * cap;
     s.ir = (double *)p; p += sizeof(double) * cap;
     s.fa = (double *)p; p += sizeof(double) * cap;
     s.fb = (double *)p; p += sizeof(double) * cap;
     s.P = (double *)p; p += sizeof(double) * cap * nep(ne);
-    s.Fnb = (double *)p; p += sizeof(double) * cap * 3;
     s.G = (double *)p; p += align16(sizeof(double) * D);
-    s.grid = (double *)p; p += sizeof(double) * nzl_cells;
-    s.red = (double *)p; p += sizeof(double) * warps * 64;
     {
         const size_t tmp_b = sizeof(double) * cap * (ng2 > 1 ? ng2 : 1), tl_b = align8(sizeof(unsigned) * tl);
         s.tmp = (double *)p;
         s.tl = (unsigned *)p;
         p += tmp_b > tl_b ? tmp_b : tl_b;
     }
-    s.h = (double *)p; p += sizeof(double) * 4 * MB_MAXH;
     s.j = (int *)p; p += align8(sizeof(int) * cap);
     s.sp = (int *)p; p += align8(sizeof(int) * cap);
-    s.raw_sp = (int *)p; p += align8(sizeof(int) * cap);
     s.blk = (int *)p; p += align8(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
     s.seg = (int *)p;
     return s;
@@ -472,11 +484,40 @@ __device__ __forceinline__ void group_reduce64(double *v, EfsSmem &s, int gwarp,
     __syncthreads();
 }
 
-/* Triplet candidates of species block (a,b) are the pairs (j,k) of the
- * rectangle seg_a x seg_b (j<k when a==b).  Rows j are dealt round-robin to
- * the group's warps; each warp appends its accepted pairs to its own region
- * [lo,hi) of the list, a row at a time, and stops before a row that might
- * not fit.  Returns the next unprocessed row of this warp. */
+/* As group_reduce64 for values already summed over the warp (lane l holds
+ * cells 2l and 2l+1, the layout of a tensor-core accumulator fragment). */
+template <int WPA>
+__device__ __forceinline__ void group_store64(double v0, double v1, EfsSmem &s, int gwarp, int lane) {
+    if (WPA == 1) {
+        s.red[2 * lane] = v0;
+        s.red[2 * lane + 1] = v1;
+        __syncwarp();
+        return;
+    }
+    s.red[gwarp * 64 + 2 * lane] = v0;
+    s.red[gwarp * 64 + 2 * lane + 1] = v1;
+    __syncthreads();
+    if (gwarp == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < WPA; w++) {
+            a += s.red[w * 64 + 2 * lane];
+            b += s.red[w * 64 + 2 * lane + 1];
+        }
+        __syncwarp();
+        s.red[2 * lane] = a;
+        s.red[2 * lane + 1] = b;
+    }
+    __syncthreads();
+}
+
+/* D(8x8) += A(8x4) B(4x8) in FP64 on the tensor cores (mma.sync m8n8k4):
+ * lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0, 1}]. */
+__device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
 /* Append the accepted candidates (j, k) of block (a, b) to this warp's
  * list region: the block's (row, col) square in row-major order, 32
  * candidates per round with every lane busy, the warps of an atom taking
@@ -516,19 +557,18 @@ __device__ __forceinline__ void run_list(const EfsSmem &s, int from, int to, int
     }
 }
 
-/* body(jj, kk, valid) with the whole warp on every round (for bodies that
- * exchange values across lanes); lanes past the end get valid = false and
- * jj = -1 - lane, so equal jj values stay adjacent */
+/* body(jj, kk, valid) with the whole warp converged on every round (for
+ * bodies that exchange values across lanes or issue warp-wide tensor-core
+ * instructions, which need all 32 lanes at one call site); lanes past the
+ * end get valid = false and jj = -1 - lane, so equal jj values stay
+ * adjacent */
 template <class Body>
 __device__ __forceinline__ void run_list_all(const EfsSmem &s, int from, int to, int lane, Body body) {
     for (int base = from; base < to; base += 32) {
         const int t = base + lane;
-        if (t < to) {
-            const unsigned pk = s.tl[t];
-            body((int)(pk & 0xffffu), (int)(pk >> 16), true);
-        } else {
-            body(-1 - lane, 0, false);
-        }
+        const bool valid = t < to;
+        const unsigned pk = valid ? s.tl[t] : 0u;
+        body(valid ? (int)(pk & 0xffffu) : -1 - lane, (int)(pk >> 16), valid);
     }
 }
 
@@ -570,6 +610,9 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
     constexpr int NZL = NZ * NLAM;
     constexpr int WARPS = WPA;
     constexpr int NEP = nep(NE);
+    /* the reference bases (<= 8 exponents x 8 angular terms): the forward
+     * grid is accumulated on the FP64 tensor cores */
+    constexpr bool TC_FWD = NE <= 8 && NZL == 8;
     extern __shared__ __align__(16) char smem_raw[];
     __shared__ mb_params Ps;
     {
@@ -584,7 +627,8 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
     const int i = blockIdx.x * APB + group;
     if (i >= A.N) return; /* whole atom groups only: no barrier spans two groups */
     const int D = P.D, ns = P.nspc, ng2 = P.ng2, ne = P.ne;
-    EfsSmem s = efs_carve(smem_raw + (size_t)group * A.smem_group, A.cap, D, NE, ng2, NE * NZL, WARPS, A.tl_cap);
+    EfsSmem s = efs_carve(smem_raw + (size_t)group * A.smem_group, A.cap, D, NE, ng2, NE * NZL, WARPS, A.tl_cap,
+                          TC_FWD);
     const int tlw = A.tl_cap / WPA, tl_lo = warp * tlw, tl_hi = tl_lo + tlw;
     int tl_pos = tl_lo, tl_whole = 1;
     const int n = A.nn[i];
@@ -592,30 +636,47 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
     const double *net = A.weights + P.w_off[s0];
 
     /* ---- stage neighbours, stably sorted by species relative to s0 ---- */
-    for (int t = tid; t < n; t += NT) s.raw_sp[t] = A.spc[A.nj[(size_t)i * A.cap + t]];
-    if (tid < 8) s.seg[tid] = 0;
     for (int t = tid; t < D; t += NT) s.G[t] = 0.0;
-    group_sync<WPA>();
-    if (tid == 0) {
+    if (warp == 0) {
+        /* counts and stable ranks per relative species from warp ballots */
+        const int *nj_i = A.nj + (size_t)i * A.cap;
+        const unsigned below = (1u << lane) - 1u;
         int cnt[4] = {0, 0, 0, 0};
-        for (int t = 0; t < n; t++) cnt[(s.raw_sp[t] - s0 + ns) % ns]++;
-        int off = 0;
-        for (int v = 0; v < 4; v++) {
-            s.seg[v] = cnt[v];
-            s.seg[4 + v] = off;
-            off += cnt[v];
+        for (int base = 0; base < n; base += 32) {
+            const int t = base + lane;
+            const int ds = t < n ? (A.spc[nj_i[t]] - s0 + ns) % ns : -1;
+#pragma unroll
+            for (int v = 0; v < 4; v++) cnt[v] += __popc(__ballot_sync(FULL, ds == v));
         }
-    }
-    group_sync<WPA>();
-    for (int t = tid; t < n; t += NT) {
-        int ds = (s.raw_sp[t] - s0 + ns) % ns, rank = 0;
-        for (int u = 0; u < t; u++) rank += ((s.raw_sp[u] - s0 + ns) % ns) == ds;
-        int dst = s.seg[4 + ds] + rank;
-        s.j[dst] = A.nj[(size_t)i * A.cap + t];
-        s.sp[dst] = s.raw_sp[t];
-        double4 dv = A.nd[(size_t)i * A.cap + t];
-        s.d[dst] = dv;
-        s.ir[dst] = 1.0 / dv.w;
+        int off[4];
+        off[0] = 0;
+#pragma unroll
+        for (int v = 1; v < 4; v++) off[v] = off[v - 1] + cnt[v - 1];
+        if (lane < 4) {
+            s.seg[lane] = cnt[lane];
+            s.seg[4 + lane] = off[lane];
+        }
+        int run[4] = {0, 0, 0, 0};
+        for (int base = 0; base < n; base += 32) {
+            const int t = base + lane;
+            const int j = t < n ? nj_i[t] : 0;
+            const int sp = t < n ? A.spc[j] : 0;
+            const int ds = t < n ? (sp - s0 + ns) % ns : -1;
+            int dst = 0;
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                const unsigned m = __ballot_sync(FULL, ds == v);
+                if (ds == v) dst = off[v] + run[v] + __popc(m & below);
+                run[v] += __popc(m);
+            }
+            if (t < n) {
+                s.j[dst] = j;
+                s.sp[dst] = sp;
+                const double4 dv = A.nd[(size_t)i * A.cap + t];
+                s.d[dst] = dv;
+                s.ir[dst] = 1.0 / dv.w;
+            }
+        }
     }
     group_sync<WPA>();
     if (tid == 0 && A.counters) atomicAdd(&A.counters[0], (unsigned long long)n);
@@ -674,9 +735,6 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
         unsigned long long nacc = 0;
         for (int a = 0; a < ns; a++)
             for (int b = a; b < ns; b++, blkid++) {
-                double acc[CELLS];
-#pragma unroll
-                for (int k = 0; k < CELLS; k++) acc[k] = 0.0;
                 /* the species of j and k are fixed within the block (neighbours are
                  * sorted by species relative to s0): hoist their parameters */
                 const int sja = (a + s0) % ns, skb = (b + s0) % ns;
@@ -692,6 +750,73 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
                            (d1.w < drc4 && d2.w < drc4 && r3s < drc4sq);
                 };
                 const double *eta12 = P.f_eta4[p12];
+                if constexpr (TC_FWD) {
+                    /* Each lane takes one listed triplet and forms its 8 exponential
+                     * factors ex[e] and 8 angular terms lz[zl]; the grid
+                     * G[e][zl] += sum_t ex_t[e] lz_t[zl] is then an outer-product
+                     * sum, done 4 triplets at a time by mma.sync m8n8k4 in FP64
+                     * with the values staged through shared memory.  The
+                     * accumulator fragment leaves lane l with cells 2l, 2l+1. */
+                    double c0 = 0.0, c1 = 0.0;
+                    double *stw = s.stage + warp * 32 * EFS_STG;
+                    auto body = [&](int jj, int kk, bool valid) {
+                        double ex[8], lz[NZL];
+#pragma unroll
+                        for (int q = 0; q < 8; q++) ex[q] = 0.0;
+#pragma unroll
+                        for (int q = 0; q < NZL; q++) lz[q] = 0.0;
+                        if (valid) {
+                            const double4 d1 = s.d[jj], d2 = s.d[kk];
+                            const double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+                            const double r3s = dx * dx + dy * dy + dz * dz;
+                            if (d1.w < rc2_01 && d1.w < rc4_01 && d2.w < rc4_02 && r3s < rc4sq_12) {
+                                nacc++;
+                                const double r3 = sqrt(r3s);
+                                const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (s.ir[jj] * s.ir[kk]);
+                                const double A3 = 2.0 * s.fa[jj] * s.fb[kk] * fcut(rc4_12, r3);
+                                angular<NZ, NLAM>(P, c, lz, nullptr);
+                                const double2 *pj = reinterpret_cast<const double2 *>(s.P + jj * NEP);
+                                const double2 *pk = reinterpret_cast<const double2 *>(s.P + kk * NEP);
+#pragma unroll
+                                for (int h = 0; h < NEP / 2; h++) {
+                                    const double2 x = pj[h], y = pk[h];
+#pragma unroll
+                                    for (int q = 0; q < 2; q++) {
+                                        const int e = 2 * h + q;
+                                        if (e < NE && e < ne)
+                                            ex[e] = A3 * (q ? x.y * y.y : x.x * y.x) * exp(-eta12[e] * r3s);
+                                    }
+                                }
+                            }
+                        }
+                        double *row = stw + lane * EFS_STG;
+#pragma unroll
+                        for (int q = 0; q < 8; q++) {
+                            row[q] = ex[q];
+                            row[8 + q] = lz[q];
+                        }
+                        __syncwarp();
+#pragma unroll
+                        for (int st = 0; st < 8; st++) {
+                            const double *r = stw + (4 * st + (lane & 3)) * EFS_STG;
+                            dmma884(c0, c1, r[lane >> 2], r[8 + (lane >> 2)]);
+                        }
+                        __syncwarp();
+                    };
+                    int *blk = s.blk + (blkid * WPA + warp) * 2;
+                    tl_whole &= for_block<WPA, true>(s, a, b, blk, 0, tl_pos, tl_lo, tl_hi, warp, lane, accept_blk, body);
+                    group_sync<WPA>();
+                    group_store64<WPA>(c0, c1, s, warp, lane);
+                    if (tid == 0) {
+                        const int base = P.ind4[a * a + b * b];
+                        for (int f = 0; f < P.ng4; f++)
+                            s.G[base + f] += s.red[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam];
+                    }
+                    group_sync<WPA>();
+                } else {
+                double acc[CELLS];
+#pragma unroll
+                for (int k = 0; k < CELLS; k++) acc[k] = 0.0;
                 auto body = [&](int jj, int kk) {
                     double4 d1 = s.d[jj], d2 = s.d[kk];
                     double dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
@@ -734,6 +859,7 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
                         }
                     }
                     group_sync<WPA>();
+                }
                 }
             }
         if (A.counters) {
@@ -1091,7 +1217,8 @@ static size_t group_bytes(const mb_model *m, int capNB, int wpa) {
     bool fast = efs_fast(m);
     int ne = fast ? 7 : MB_MAXE;
     int cells = fast ? 7 * 8 : MB_MAXE * 8 * 4;
-    return (efs_smem_bytes(capNB, m->P.D, ne, m->P.ng2, cells, wpa, tl_entries(capNB, wpa)) + 15) & ~(size_t)15;
+    return (efs_smem_bytes(capNB, m->P.D, ne, m->P.ng2, cells, wpa, tl_entries(capNB, wpa), fast ? 1 : 0) + 15) &
+           ~(size_t)15;
 }
 
 extern "C" size_t mbk_efs_smem(const mb_model *m, int capNB, int shape) {

@@ -33,7 +33,11 @@ constexpr int BMAXNB = 96;
 constexpr int BMAXDOF = 3 * BMAXN + 9;
 constexpr int BMAXD = 288;
 constexpr int BTL = 1024;
-constexpr int BWARPS = 4;
+/* warps per structure: 4 (three structures per SM) for large populations,
+ * 12 (one structure per SM, a third of the evaluation latency) when the
+ * population fits the SMs in about two rounds and its slowest structure
+ * decides the time */
+constexpr int BWARPS_WIDE = 12;
 constexpr int BIMG = 4; /* image shifts a lane holds in the fast neighbour search (128 images) */
 constexpr int BNE = 7, BNZ = 4, BNLAM = 2, BNZL = 8, BCELLS = 64;
 
@@ -85,20 +89,21 @@ struct WarpWS {
     int seg[8];
 };
 
+template <int W>
 struct BShared {
     double L[9], R[9];
     double xc[BMAXN * 3];
     double ea[BMAXN], eu[BMAXN];
     double x[BMAXDOF], g[BMAXDOF], p[BMAXDOF], xt[BMAXDOF], gt[BMAXDOF], xa[BMAXDOF], ga[BMAXDOF], hy[BMAXDOF];
-    double vir[BWARPS][6];
+    double vir[W][6];
     double uvir[6];
-    double red[BWARPS * 32];
+    double red[W * 32];
     double scal[24];
     float F[BMAXN * 3];
     int spc[BMAXN];
     int nn[BMAXN];
     int s, N, ndof, flag, cmd, first;
-    WarpWS ws[BWARPS];
+    WarpWS ws[W];
 };
 
 /* ---------------- small helpers ---------------- */
@@ -186,19 +191,21 @@ __device__ __forceinline__ void warp_reduce64f(float *v, int lane) {
 }
 
 /* CTA-wide sum of one double per thread (all threads get the result) */
-__device__ double cta_sum(BShared &sh, double v) {
+template <int W>
+__device__ double cta_sum(BShared<W> &sh, double v) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     v = bsum(v);
     __syncthreads();
     if (lane == 0) sh.red[w] = v;
     __syncthreads();
     double t = 0.0;
-    for (int k = 0; k < BWARPS; k++) t += sh.red[k];
+    for (int k = 0; k < W; k++) t += sh.red[k];
     __syncthreads();
     return t;
 }
 
-__device__ double cta_max(BShared &sh, double v) {
+template <int W>
+__device__ double cta_max(BShared<W> &sh, double v) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULLM, v, o));
@@ -206,7 +213,7 @@ __device__ double cta_max(BShared &sh, double v) {
     if (lane == 0) sh.red[w] = v;
     __syncthreads();
     double t = 0.0;
-    for (int k = 0; k < BWARPS; k++) t = fmax(t, sh.red[k]);
+    for (int k = 0; k < W; k++) t = fmax(t, sh.red[k]);
     __syncthreads();
     return t;
 }
@@ -240,7 +247,8 @@ __device__ __forceinline__ bool tgate(const BParams &P, const WarpWS &ws, int s0
 
 /* ---------------- one atom: descriptors, MLP, reverse pass (FP32) ---------------- */
 
-__device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const float4 *nbd, const int *nbj,
+template <int W>
+__device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, const float4 *nbd, const int *nbj,
                           double *virw) {
     const BParams &P = *A.P;
     const int lane = threadIdx.x & 31;
@@ -655,7 +663,8 @@ __device__ void atom_pass(const BArgs &A, BShared &sh, WarpWS &ws, int i, const 
 /* ---------------- one evaluation of the structure at DOF vector dof ---------------- */
 
 /* Returns H; gradient into gout; sh.scal[1] = max|F|, sh.scal[2] = max|U-pV|/N. */
-__device__ double evaluate(const BArgs &A, BShared &sh, const double *dof, double *gout) {
+template <int W>
+__device__ double evaluate(const BArgs &A, BShared<W> &sh, const double *dof, double *gout) {
     const BParams &P = *A.P;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, N = sh.N, rlxt = A.rlxt;
     float4 *nbd = A.nbd + (size_t)blockIdx.x * BMAXN * BMAXNB;
@@ -700,7 +709,7 @@ __device__ double evaluate(const BArgs &A, BShared &sh, const double *dof, doubl
             shz[t] = c0 * sh.L[2] + c1 * sh.L[5] + c2 * sh.L[8];
             if (c0 == 0 && c1 == 0 && c2 == 0) zero |= 1u << t;
         }
-        for (int i = w; i < N; i += BWARPS) {
+        for (int i = w; i < N; i += W) {
             int count = 0;
             const double xi0 = sh.xc[3 * i], xi1 = sh.xc[3 * i + 1], xi2 = sh.xc[3 * i + 2];
             for (int j = 0; j < N; j++) {
@@ -727,7 +736,7 @@ __device__ double evaluate(const BArgs &A, BShared &sh, const double *dof, doubl
             }
         }
     } else
-    for (int i = w; i < N; i += BWARPS) {
+    for (int i = w; i < N; i += W) {
         int count = 0;
         const double xi0 = sh.xc[3 * i], xi1 = sh.xc[3 * i + 1], xi2 = sh.xc[3 * i + 2];
         for (int base = 0; base < N * nimg; base += 32) {
@@ -762,7 +771,7 @@ __device__ double evaluate(const BArgs &A, BShared &sh, const double *dof, doubl
     __syncthreads();
     /* descriptors, MLP and forces, one warp per atom */
     double virw[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = w; i < N; i += BWARPS) atom_pass(A, sh, sh.ws[w], i, nbd, nbj, virw);
+    for (int i = w; i < N; i += W) atom_pass(A, sh, sh.ws[w], i, nbd, nbj, virw);
     if (lane == 0)
         for (int k = 0; k < 6; k++) sh.vir[w][k] = virw[k];
     __syncthreads();
@@ -779,7 +788,7 @@ __device__ double evaluate(const BArgs &A, BShared &sh, const double *dof, doubl
         sh.scal[3] = 4.0 * 1.1920929e-7 * mag;
         for (int k = 0; k < 6; k++) {
             U[k] = 0.0;
-            for (int ww = 0; ww < BWARPS; ww++) U[k] += sh.vir[ww][k];
+            for (int ww = 0; ww < W; ww++) U[k] += sh.vir[ww][k];
         }
         const double *L = sh.L;
         double V = fabs(L[0] * L[4] * L[8] + L[2] * L[3] * L[7] + L[1] * L[5] * L[6] - L[0] * L[5] * L[7] -
@@ -863,9 +872,10 @@ __device__ void vcopy(double *dst, const double *src, int n) {
     for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
 }
 
-__global__ void __launch_bounds__(BWARPS * 32) k_relax_batch(BArgs A) {
+template <int W>
+__global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
     extern __shared__ __align__(16) char smem_raw[];
-    BShared &sh = *reinterpret_cast<BShared *>(smem_raw);
+    BShared<W> &sh = *reinterpret_cast<BShared<W> *>(smem_raw);
     const int tid = threadIdx.x;
     double *H = A.hmat + (size_t)blockIdx.x * BMAXDOF * BMAXDOF;
     const double rho = 0.01, tau1 = 9.0, tau2 = 0.05, tau3 = 0.5;
@@ -1132,6 +1142,15 @@ static int build_bparams(const mb_model *m, BParams *B, float **w_out, size_t *w
     return 0;
 }
 
+/* launch geometry of k_relax_batch<W> on this device */
+template <int W>
+static cudaError_t batch_config(int *per) {
+    const size_t smem = sizeof(BShared<W>);
+    cudaError_t e = cudaFuncSetAttribute(k_relax_batch<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_relax_batch<W>, W * 32, smem);
+}
+
 extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const int *d_off, const int *d_spc,
                                const int *d_order, double *d_lat, double *d_x, double p_ev, double urep, int rlxt, int mitr, double fmax,
                                double *d_H, int *d_iters, int *d_status, void *stream, long long *evals_out,
@@ -1144,10 +1163,11 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    size_t smem = sizeof(BShared);
-    cudaError_t e = cudaFuncSetAttribute(k_relax_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    /* a population that fits the SMs in about two rounds is bound by its
+     * slowest structure: give each structure a whole SM */
+    const int wide = S <= 2 * sms;
+    cudaError_t e = wide ? batch_config<BWARPS_WIDE>(&per) : batch_config<4>(&per);
     if (e != cudaSuccess) { free(hw); return (int)e; }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_batch, BWARPS * 32, smem);
     if (per < 1) { free(hw); return (int)cudaErrorInvalidConfiguration; }
     int grid = sms * per < S ? sms * per : S;
     BParams *dp = nullptr;
@@ -1178,7 +1198,10 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
         a.lat = d_lat; a.x = d_x; a.H = d_H; a.iters = d_iters; a.status = d_status;
         a.P = dp; a.W = dw; a.queue = queue; a.hmat = hm; a.nbd = nbd; a.nbj = nbj; a.evals = evals;
         cudaEventRecord(e0, st);
-        k_relax_batch<<<grid, BWARPS * 32, smem, st>>>(a);
+        if (wide)
+            k_relax_batch<BWARPS_WIDE><<<grid, BWARPS_WIDE * 32, sizeof(BShared<BWARPS_WIDE>), st>>>(a);
+        else
+            k_relax_batch<4><<<grid, 4 * 32, sizeof(BShared<4>), st>>>(a);
         cudaEventRecord(e1, st);
         e = cudaGetLastError();
     }

@@ -265,7 +265,8 @@ def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs
     t0 = time.perf_counter()
     pred = sur.screen(gen)
     kept = keep_best(pred, keep)
-    pot.relax_batch([gen[i] for i in kept], urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
+    t_pred = time.perf_counter() - t0
+    rk = pot.relax_batch([gen[i] for i in kept], urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
     t_scr = time.perf_counter() - t0
     e0 = np.array([pot.energy(s["X"], s["LAT"], s["atmn"], ND=3, NM=300, urep=urep)["H"] for s in gen]) / nat
     sur.close()
@@ -274,6 +275,7 @@ def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs
             "recall_top10": recall(pred, truth, keep), "recall_top10_by_unrelaxed_energy": recall(e0, truth, keep),
             "recall_top10_random_expectation": keep,
             "generation_s_relax_all": t_all, "generation_s_screened": t_scr, "speedup": t_all / t_scr,
+            "screen_s": t_pred, "relax_all_kernel_ms": ra["ms"], "relax_kept_kernel_ms": rk["ms"],
             "train_data_relax_s": t_data, "fit_s": t_fit, "epochs": epochs, "final_loss": float(loss[-1]),
             "judge": "batched relax of every offspring (FP32 descriptors/MLP, FP64 BFGS)"}
 

@@ -18,6 +18,7 @@
  * A structure stops when max |F| < fmax and max |U - pV| / N < fmax.
  */
 #include <cuda_runtime.h>
+#include <stdlib.h>
 #include <math_constants.h>
 #include <stdint.h>
 
@@ -33,10 +34,13 @@ constexpr int BMAXNB = 96;
 constexpr int BMAXDOF = 3 * BMAXN + 9;
 constexpr int BMAXD = 288;
 constexpr int BTL = 1024;
-/* warps per structure: 4 (three structures per SM) for large populations,
- * 12 (one structure per SM, a third of the evaluation latency) when the
- * population fits the SMs in about two rounds and its slowest structure
- * decides the time */
+/* warps per structure: 12 (one structure per SM) by default, 4 (three
+ * structures per SM) on request.  Both hold the 12 warps per SM that 168
+ * registers a thread allow; the wide CTA finishes each structure in about a
+ * third of the time, which bounds a launch through its slowest structure,
+ * and runs the per-structure FP64 work (BFGS vectors, list builds) on three
+ * times the threads, so it is also the faster one for large populations
+ * (20000 Cu-Pd-Ag offspring of 16-48 atoms: 9.7 s against 14.9 s) */
 constexpr int BWARPS_WIDE = 12;
 constexpr int BIMG = 4; /* image shifts a lane holds in the fast neighbour search (128 images) */
 constexpr int BNE = 7, BNZ = 4, BNLAM = 2, BNZL = 8, BCELLS = 64;
@@ -1163,9 +1167,12 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    /* a population that fits the SMs in about two rounds is bound by its
-     * slowest structure: give each structure a whole SM */
-    const int wide = S <= 2 * sms;
+    int wide = 1;
+    {
+        /* MAISE_B200_BATCH_WARPS=4 selects the narrow CTA (A/B timing) */
+        const char *fw = getenv("MAISE_B200_BATCH_WARPS");
+        if (fw) wide = atoi(fw) != 4;
+    }
     cudaError_t e = wide ? batch_config<BWARPS_WIDE>(&per) : batch_config<4>(&per);
     if (e != cudaSuccess) { free(hw); return (int)e; }
     if (per < 1) { free(hw); return (int)cudaErrorInvalidConfiguration; }

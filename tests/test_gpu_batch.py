@@ -30,9 +30,18 @@ def _nat(pop):
     return np.array([len(s["atmn"]) for s in pop])
 
 
-def test_fp32_energy_of_start_structures_matches_fp64(mgca):
+@pytest.fixture(params=["12", "4"], ids=["12warps", "4warps"])
+def width(request, monkeypatch):
+    """Warps per structure of the batched kernel (the library reads
+    MAISE_B200_BATCH_WARPS at every launch; 12 is the default)."""
+    monkeypatch.setenv("MAISE_B200_BATCH_WARPS", request.param)
+    return int(request.param)
+
+
+def test_fp32_energy_of_start_structures_matches_fp64(mgca, width):
     """With no iterations the batched path reports each structure's enthalpy
-    from its FP32 evaluation: within 1e-5 eV/atom of the FP64 path."""
+    from its FP32 evaluation: within 1e-5 eV/atom of the FP64 path, with
+    either CTA width."""
     pot, pop = mgca
     r = pot.relax_batch(pop, urep=UREP, rlxt=3, mitr=0, fmax=FMAX)
     for k, s in enumerate(pop):
@@ -42,7 +51,7 @@ def test_fp32_energy_of_start_structures_matches_fp64(mgca):
 
 
 @pytest.mark.parametrize("rlxt", [2, 3])
-def test_batched_minima_are_fp64_minima(mgca, rlxt):
+def test_batched_minima_are_fp64_minima(mgca, rlxt, width):
     pot, pop = mgca
     r = pot.relax_batch(pop, urep=UREP, rlxt=rlxt, mitr=1000, fmax=FMAX)
     conv = np.flatnonzero(r["status"] == 0)

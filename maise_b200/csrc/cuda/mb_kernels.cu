@@ -518,24 +518,46 @@ __device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double
                  : "d"(a), "d"(b));
 }
 
+/* Candidates of block (a, b): the na x nb square for a != b; for a == b
+ * only the strict upper triangle (col > row), enumerated directly up to 256
+ * neighbours of the species (the square with the lower half skipped above) */
+__device__ __forceinline__ bool block_tri(const EfsSmem &s, int a, int b) { return a == b && s.seg[a] <= 256; }
+__device__ __forceinline__ int block_candidates(const EfsSmem &s, int a, int b) {
+    const int na = s.seg[a], nb = s.seg[b];
+    return block_tri(s, a, b) ? na * (na - 1) / 2 : na * nb;
+}
+
 /* Append the accepted candidates (j, k) of block (a, b) to this warp's
- * list region: the block's (row, col) square in row-major order, 32
- * candidates per round with every lane busy, the warps of an atom taking
- * every WPA-th round (row = (c + 0.5) / nb in FP32 is exact: the fraction
- * stays >= 0.5 / nb away from an integer).  Returns the next candidate
+ * list region in row-major order, 32 candidates per round with every lane
+ * busy, the warps of an atom taking every WPA-th round.  Square: row =
+ * (c + 0.5) / nb in FP32 is exact (the fraction stays >= 0.5 / nb away from
+ * an integer).  Triangle: row r starts at r (2 na - r - 1) / 2, inverted
+ * with one FP32 square root and corrected by one row either way (exact for
+ * na <= 256 under +-2 ulp of sqrt error).  Returns the next candidate
  * index; stops early when the region is full. */
 template <int WPA, class Accept>
 __device__ __forceinline__ int fill_chunks(const EfsSmem &s, int a, int b, int c, int &pos, int hi, int lane,
                                            Accept accept) {
     const int na = s.seg[a], nb = s.seg[b], oa = s.seg[4 + a], ob = s.seg[4 + b];
-    const int C = na * nb;
-    const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f;
+    const bool tri = block_tri(s, a, b);
+    const int C = block_candidates(s, a, b);
+    const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f, tb = (float)(2 * na - 1);
     for (; c < C && pos + 32 <= hi; c += 32 * WPA) {
         const int cc = c + lane;
         bool ok = false;
         int jj = 0, kk = 0;
         if (cc < C) {
-            const int r = __float2int_rz(((float)cc + 0.5f) * inv_nb), col = cc - r * nb;
+            int r, col;
+            if (tri) {
+                r = __float2int_rz(0.5f * (tb - sqrtf(tb * tb - 8.0f * (float)cc)));
+                if ((r + 1) * (2 * na - r - 2) / 2 <= cc) r++;
+                else if (r * (2 * na - r - 1) / 2 > cc) r--;
+                r = min(max(r, 0), na - 2);
+                col = min(max(cc - r * (2 * na - r - 1) / 2 + r + 1, r + 1), na - 1);
+            } else {
+                r = __float2int_rz(((float)cc + 0.5f) * inv_nb);
+                col = cc - r * nb;
+            }
             jj = oa + r;
             kk = ob + col;
             ok = (a != b || col > r) && accept(jj, kk);
@@ -554,6 +576,45 @@ __device__ __forceinline__ void run_list(const EfsSmem &s, int from, int to, int
     for (int t = from + lane; t < to; t += 32) {
         const unsigned pk = s.tl[t];
         body((int)(pk & 0xffffu), (int)(pk >> 16));
+    }
+}
+
+/* body(jj, kk) -> the entry's force on neighbour j, over list entries
+ * [from, to): each lane takes a contiguous run of K entries (K odd, so that
+ * the lanes' reads of the list fall in distinct banks).  The list runs row
+ * by row, so a lane's entries mostly share j: their j-side forces are summed
+ * in registers and added to Fnb once per change of j.  The body must not
+ * exchange values across lanes (lanes leave the loop at different times). */
+template <class Body>
+__device__ __forceinline__ void run_list_runs(const EfsSmem &s, int from, int to, int lane, Body body) {
+    int K = (to - from + 31) >> 5;
+    if (K > 0) K |= 1;
+    const int t0 = from + lane * K;
+    int cj = -1;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int step = 0; step < K; step++) {
+        const int t = t0 + step;
+        if (t >= to) break;
+        const unsigned pk = s.tl[t];
+        const int jj = (int)(pk & 0xffffu), kk = (int)(pk >> 16);
+        if (jj != cj) {
+            if (cj >= 0) {
+                atomicAdd(&s.Fnb[3 * cj], -sx);
+                atomicAdd(&s.Fnb[3 * cj + 1], -sy);
+                atomicAdd(&s.Fnb[3 * cj + 2], -sz);
+            }
+            cj = jj;
+            sx = sy = sz = 0.0;
+        }
+        const double3 g = body(jj, kk);
+        sx += g.x;
+        sy += g.y;
+        sz += g.z;
+    }
+    if (cj >= 0) {
+        atomicAdd(&s.Fnb[3 * cj], -sx);
+        atomicAdd(&s.Fnb[3 * cj + 1], -sy);
+        atomicAdd(&s.Fnb[3 * cj + 2], -sz);
     }
 }
 
@@ -576,25 +637,32 @@ __device__ __forceinline__ void run_list_all(const EfsSmem &s, int from, int to,
  * entries [blk[0], blk[1]) when `reuse` and filling (in rounds when the
  * region overflows) otherwise.  Records the range for later reuse and
  * returns 0 if the region overflowed (then the range is not reusable). */
-template <int WPA, bool ALL = false, class Accept, class Body>
+/* how for_block runs a body over list entries */
+enum { RUN_LANES = 0, RUN_CONVERGED = 1, RUN_RUNS = 2 };
+
+template <int RUN, class Body>
+__device__ __forceinline__ void run_entries(const EfsSmem &s, int from, int to, int lane, Body body) {
+    if constexpr (RUN == RUN_CONVERGED)
+        run_list_all(s, from, to, lane, body);
+    else if constexpr (RUN == RUN_RUNS)
+        run_list_runs(s, from, to, lane, body);
+    else
+        run_list(s, from, to, lane, body);
+}
+
+template <int WPA, int RUN = RUN_LANES, class Accept, class Body>
 __device__ __forceinline__ int for_block(const EfsSmem &s, int a, int b, int *blk, int reuse, int &pos, int lo,
                                          int hi, int warp, int lane, Accept accept, Body body) {
     if (reuse) {
-        if constexpr (ALL)
-            run_list_all(s, blk[0], blk[1], lane, body);
-        else
-            run_list(s, blk[0], blk[1], lane, body);
+        run_entries<RUN>(s, blk[0], blk[1], lane, body);
         return 1;
     }
     int start = pos, c = warp * 32, whole = 1;
-    const int C = s.seg[a] * s.seg[b];
+    const int C = block_candidates(s, a, b);
     for (;;) {
         const int from = pos;
         c = fill_chunks<WPA>(s, a, b, c, pos, hi, lane, accept);
-        if constexpr (ALL)
-            run_list_all(s, from, pos, lane, body);
-        else
-            run_list(s, from, pos, lane, body);
+        run_entries<RUN>(s, from, pos, lane, body);
         __syncwarp();
         if (c >= C) break;
         whole = 0; /* region full: restart it for the next round */
@@ -605,8 +673,12 @@ __device__ __forceinline__ int for_block(const EfsSmem &s, int a, int b, int *bl
     return whole;
 }
 
+/* The 4-atoms-per-CTA shape holds two CTAs per SM (its shared memory per
+ * atom decides that), so it may use up to 256 registers a thread: asking for
+ * two blocks per SM lets it run without spills instead of the register
+ * budget of three. */
 template <int NE, int NZ, int NLAM, int WPA, int APB>
-__global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
+__global__ void __launch_bounds__(WPA * 32 * APB, APB >= 4 ? 2 : 1) k_efs(EfsArgs A) {
     constexpr int NZL = NZ * NLAM;
     constexpr int WARPS = WPA;
     constexpr int NEP = nep(NE);
@@ -804,7 +876,7 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
                         __syncwarp();
                     };
                     int *blk = s.blk + (blkid * WPA + warp) * 2;
-                    tl_whole &= for_block<WPA, true>(s, a, b, blk, 0, tl_pos, tl_lo, tl_hi, warp, lane, accept_blk, body);
+                    tl_whole &= for_block<WPA, RUN_CONVERGED>(s, a, b, blk, 0, tl_pos, tl_lo, tl_hi, warp, lane, accept_blk, body);
                     group_sync<WPA>();
                     group_store64<WPA>(c0, c1, s, warp, lane);
                     if (tid == 0) {
@@ -974,15 +1046,13 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
                     for (int f = 0; f < P.ng4; f++)
                         s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam] += s.G[base + f];
                 group_sync<WPA>();
-                auto body = [&](int jj, int kk, bool valid) {
-                    double g1x = 0.0, g1y = 0.0, g1z = 0.0, g2x = 0.0, g2y = 0.0, g2z = 0.0;
-                    bool on = false;
-                    if (valid) {
-                    double4 d1 = s.d[jj], d2 = s.d[kk];
-                    double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
-                    double r3s = wx * wx + wy * wy + wz * wz;
-                    on = d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq;
-                    if (on) {
+                /* returns the entry's force on neighbour j; run_list_runs sums
+                 * those per lane and adds them once per change of j */
+                auto body = [&](int jj, int kk) -> double3 {
+                    const double4 d1 = s.d[jj], d2 = s.d[kk];
+                    const double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
+                    const double r3s = wx * wx + wy * wy + wz * wz;
+                    if (!(d1.w < P.d_rc4 && d2.w < P.d_rc4 && r3s < P.d_rc4sq)) return make_double3(0.0, 0.0, 0.0);
                     double r3 = sqrt(r3s);
                     double r1 = d1.w, r2 = d2.w, ir1 = s.ir[jj], ir2 = s.ir[kk], ir3 = 1.0 / r3;
                     double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
@@ -1023,42 +1093,20 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs(EfsArgs A) {
                     double Tc = Af * Qc;
                     double a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
                     double a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
-                    g1x = a11 * d1.x + a12 * d2.x - a3 * wx;
-                    g1y = a11 * d1.y + a12 * d2.y - a3 * wy;
-                    g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
-                    g2x = a22 * d2.x + a12 * d1.x + a3 * wx;
-                    g2y = a22 * d2.y + a12 * d1.y + a3 * wy;
-                    g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
-                    }
-                    }
+                    const double g1x = a11 * d1.x + a12 * d2.x - a3 * wx;
+                    const double g1y = a11 * d1.y + a12 * d2.y - a3 * wy;
+                    const double g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
+                    const double g2x = a22 * d2.x + a12 * d1.x + a3 * wx;
+                    const double g2y = a22 * d2.y + a12 * d1.y + a3 * wy;
+                    const double g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
                     fi[0] += g1x + g2x; fi[1] += g1y + g2y; fi[2] += g1z + g2z;
-                    if (on) {
-                        atomicAdd(&s.Fnb[3 * kk], -g2x);
-                        atomicAdd(&s.Fnb[3 * kk + 1], -g2y);
-                        atomicAdd(&s.Fnb[3 * kk + 2], -g2z);
-                    }
-                    /* j side: the list runs row by row, so lanes with the same j are
-                     * adjacent; sum each run and add it with one atomic */
-#pragma unroll
-                    for (int off = 1; off < 32; off <<= 1) {
-                        const double ox = __shfl_down_sync(FULL, g1x, off), oy = __shfl_down_sync(FULL, g1y, off),
-                                     oz = __shfl_down_sync(FULL, g1z, off);
-                        const int ok = __shfl_down_sync(FULL, jj, off);
-                        if (lane + off < 32 && ok == jj) {
-                            g1x += ox;
-                            g1y += oy;
-                            g1z += oz;
-                        }
-                    }
-                    const int prev = __shfl_up_sync(FULL, jj, 1);
-                    if (valid && (lane == 0 || prev != jj)) {
-                        atomicAdd(&s.Fnb[3 * jj], -g1x);
-                        atomicAdd(&s.Fnb[3 * jj + 1], -g1y);
-                        atomicAdd(&s.Fnb[3 * jj + 2], -g1z);
-                    }
+                    atomicAdd(&s.Fnb[3 * kk], -g2x);
+                    atomicAdd(&s.Fnb[3 * kk + 1], -g2y);
+                    atomicAdd(&s.Fnb[3 * kk + 2], -g2z);
+                    return make_double3(g1x, g1y, g1z);
                 };
                 int *blk = s.blk + (blkid * WPA + warp) * 2;
-                for_block<WPA, true>(s, a, b, blk, reuse, tl_pos, tl_lo, tl_hi, warp, lane, accept_union, body);
+                for_block<WPA, RUN_RUNS>(s, a, b, blk, reuse, tl_pos, tl_lo, tl_hi, warp, lane, accept_union, body);
                 group_sync<WPA>();
             }
     }

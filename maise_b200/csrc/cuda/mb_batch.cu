@@ -17,6 +17,7 @@
  *   - the gradient of cdfunc_gsl (src/cmin.c:107-166) in FP64.
  * A structure stops when max |F| < fmax and max |U - pV| / N < fmax.
  */
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdlib.h>
 #include <math_constants.h>
@@ -107,6 +108,9 @@ struct BShared {
     int spc[BMAXN];
     int nn[BMAXN];
     int s, N, ndof, flag, cmd, first;
+    /* posted by the cluster's rank 0 before each evaluation: structure
+     * (-1: exit) and which DOF vector (0: x, 1: xt) the other ranks copy */
+    int cmd_s, cmd_dof;
     WarpWS ws[W];
 };
 
@@ -192,6 +196,24 @@ __device__ __forceinline__ void warp_reduce64f(float *v, int lane) {
             v[k] = keep + __shfl_xor_sync(FULLM, send, off);
         }
     }
+}
+
+/* Sum of 16 per-lane accumulators across the warp: four halving steps
+ * (8 + 4 + 2 + 1 exchanges) leave lanes l and l^1 with partial sums of cell
+ * (l >> 1) & 15, and one more exchange completes it in both. */
+__device__ __forceinline__ float warp_reduce16f(float *v, int lane) {
+#pragma unroll
+    for (int step = 0; step < 4; step++) {
+        const int off = 16 >> step, half = 8 >> step;
+        const bool upper = (lane & off) != 0;
+#pragma unroll
+        for (int k = 0; k < half; k++) {
+            const float send = upper ? v[k] : v[k + half];
+            const float keep = upper ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(FULLM, send, off);
+        }
+    }
+    return v[0] + __shfl_xor_sync(FULLM, v[0], 1);
 }
 
 /* CTA-wide sum of one double per thread (all threads get the result) */
@@ -297,12 +319,11 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
     }
     __syncwarp();
 
-    /* forward pairs: G2 sums per relative species (lane accumulators, warp sums) */
-    float g2acc[3][16];
+    /* forward pairs: G2 sums per relative species v and function f in lane
+     * accumulators (cell 16 v + f; cells 48-63 stay zero), then warp sums */
+    float g2acc[64];
 #pragma unroll
-    for (int v = 0; v < 3; v++)
-#pragma unroll
-        for (int f = 0; f < 16; f++) g2acc[v][f] = 0.0f;
+    for (int k = 0; k < 64; k++) g2acc[k] = 0.0f;
     double eu = 0.0;
     for (int t = lane; t < n; t += 32) {
         float4 dv = ws.d[t];
@@ -321,7 +342,7 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
                     float val = fa * expf(-P.f_eta2[p][f] * (x * x));
 #pragma unroll
                     for (int v = 0; v < 3; v++)
-                        if (v == ds1) g2acc[v][f] += val;
+                        if (v == ds1) g2acc[16 * v + f] += val;
                 }
             }
         }
@@ -330,13 +351,14 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
             if (rd < R) eu += A.urep * 0.5 * (1.0 + cospi(rd / R)) * R / rd;
         }
     }
+    /* summed across the warp by recursive halving: lane l ends with cells
+     * 2l and 2l+1 */
+    warp_reduce64f(g2acc, lane);
 #pragma unroll
-    for (int v = 0; v < 3; v++)
-#pragma unroll
-        for (int f = 0; f < 16; f++) {
-            float t = bsumf(g2acc[v][f]);
-            if (lane == 0 && v < ns && f < ng2) ws.G[P.ind2[v] + f] = t;
-        }
+    for (int h = 0; h < 2; h++) {
+        const int cell = 2 * lane + h, v = cell >> 4, f = cell & 15;
+        if (v < ns && f < ng2) ws.G[P.ind2[v] + f] = g2acc[h];
+    }
     eu = bsum(eu);
     if (lane == 0) sh.eu[i] = eu;
     __syncwarp();
@@ -360,10 +382,15 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
 #pragma unroll
             for (int e = 0; e < BNE; e++) eta12[e] = P.f_eta4[p12][e];
             /* candidates (row, col) of the block in row-major order, 32 per
-             * round with every lane busy: row = (c + 0.5) / nb in FP32 is exact
-             * (the fraction stays >= 0.5 / nb from an integer) */
-            const int C = na * nb;
-            const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f;
+             * round with every lane busy.  Mixed blocks: all na x nb, row =
+             * (c + 0.5) / nb in FP32 is exact (the fraction stays >= 0.5 / nb
+             * from an integer).  Same-species blocks: only col > row; row r
+             * starts at r (2 na - r - 1) / 2, inverted with one square root
+             * and corrected by one row either way (exact for na <= 96 under
+             * +-2 ulp of sqrt error) */
+            const bool tri = a == b;
+            const int C = tri ? na * (na - 1) / 2 : na * nb;
+            const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f, tb = (float)(2 * na - 1);
             int c = 0;
             for (;;) {
                 int from = tl_pos;
@@ -372,16 +399,24 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
                     bool ok = false;
                     int jj = 0, kk = 0;
                     if (cc < C) {
-                        const int r = __float2int_rz(((float)cc + 0.5f) * inv_nb), col = cc - r * nb;
+                        int r, col;
+                        if (tri) {
+                            r = __float2int_rz(0.5f * (tb - sqrtf(tb * tb - 8.0f * (float)cc)));
+                            if ((r + 1) * (2 * na - r - 2) / 2 <= cc) r++;
+                            else if (r * (2 * na - r - 1) / 2 > cc) r--;
+                            r = min(max(r, 0), na - 2);
+                            col = min(max(cc - r * (2 * na - r - 1) / 2 + r + 1, r + 1), na - 1);
+                        } else {
+                            r = __float2int_rz(((float)cc + 0.5f) * inv_nb);
+                            col = cc - r * nb;
+                        }
                         jj = oa + r;
                         kk = ob + col;
-                        if (a != b || col > r) {
-                            const float4 d1 = ws.d[jj], d2 = ws.d[kk];
-                            const float dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
-                            const float r3s = dx * dx + dy * dy + dz * dz;
-                            ok = (d1.w < rc2_01 && d1.w < rc4_01 && d2.w < rc4_02 && r3s < rc4sq_12) ||
-                                 (d1.w < drc4 && d2.w < drc4 && r3s < drc4sq);
-                        }
+                        const float4 d1 = ws.d[jj], d2 = ws.d[kk];
+                        const float dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
+                        const float r3s = dx * dx + dy * dy + dz * dz;
+                        ok = (d1.w < rc2_01 && d1.w < rc4_01 && d2.w < rc4_02 && r3s < rc4sq_12) ||
+                             (d1.w < drc4 && d2.w < drc4 && r3s < drc4sq);
                     }
                     const unsigned m = __ballot_sync(FULLM, ok);
                     if (ok) ws.tl[tl_pos + __popc(m & ((1u << lane) - 1u))] = (unsigned)jj | ((unsigned)kk << 16);
@@ -443,11 +478,27 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
     const float *off = net, *W0 = off + D, *b0 = W0 + h1 * D, *W1 = b0 + h1, *b1 = W1 + h2 * h1, *W2 = b1 + h2,
                 *b2 = W2 + h2;
     float *H1 = ws.h, *Dl1 = ws.h + 2 * MB_MAXH;
-    for (int m = 0; m < h1; m++) {
-        float acc = 0.0f;
-        for (int l = lane; l < D; l += 32) acc += (ws.G[l] - off[l]) * W0[m * D + l];
-        acc = bsumf(acc);
-        if (lane == 0) H1[m] = tanhf(b0[m] + acc);
+    if (h1 <= 16) {
+        /* every hidden unit's partial sum in each lane, then one reduction */
+        float acc[16];
+#pragma unroll
+        for (int m = 0; m < 16; m++) acc[m] = 0.0f;
+        for (int l = lane; l < D; l += 32) {
+            const float x = ws.G[l] - off[l];
+#pragma unroll
+            for (int m = 0; m < 16; m++)
+                if (m < h1) acc[m] += x * W0[m * D + l];
+        }
+        const float tot = warp_reduce16f(acc, lane);
+        const int cell = (lane >> 1) & 15;
+        if (!(lane & 1) && cell < h1) H1[cell] = tanhf(b0[cell] + tot);
+    } else {
+        for (int m = 0; m < h1; m++) {
+            float acc = 0.0f;
+            for (int l = lane; l < D; l += 32) acc += (ws.G[l] - off[l]) * W0[m * D + l];
+            acc = bsumf(acc);
+            if (lane == 0) H1[m] = tanhf(b0[m] + acc);
+        }
     }
     __syncwarp();
     float v = 0.0f;
@@ -546,89 +597,87 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
                     lo = 0;
                     __syncwarp();
                 }
-                for (int base = lo; base < hi; base += 32) {
-                    /* lanes take consecutive list entries; the list runs row by row,
-                     * so lanes with the same j are adjacent (key -1-lane past the end) */
-                    const int t = base + lane;
-                    int jj = -1 - lane, kk = 0;
-                    bool on = false;
-                    float g1x = 0.0f, g1y = 0.0f, g1z = 0.0f, g2x = 0.0f, g2y = 0.0f, g2z = 0.0f;
-                    if (t < hi) {
-                    const unsigned pk = ws.tl[t];
-                    jj = pk & 0xffff;
-                    kk = pk >> 16;
-                    float4 d1 = ws.d[jj], d2 = ws.d[kk];
-                    float wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
-                    float r3s = wx * wx + wy * wy + wz * wz, r3 = sqrtf(r3s);
-                    on = d1.w < drc4 && d2.w < drc4 && r3s < drc4sq;
-                    if (on) {
-                    float r1 = d1.w, r2 = d2.w, ir1 = ws.ir[jj], ir2 = ws.ir[kk], ir3 = 1.0f / r3;
-                    float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
-                    float f3, df3;
-                    fcutf_d(drc4, r3, f3, df3);
-                    float f1 = ws.fa[jj], df1 = ws.fb[jj], f2 = ws.fa[kk], df2 = ws.fb[kk];
-                    float lz[BNZL], lzp[BNZL];
-                    angularf(P, c, lz, lzp);
-                    float Q = 0.0f, Qe = 0.0f, Qc = 0.0f;
-                    const float4 *pj = reinterpret_cast<const float4 *>(ws.P + jj * 8);
-                    const float4 *pk4 = reinterpret_cast<const float4 *>(ws.P + kk * 8);
-                    const float4 ja = pj[0], jb = pj[1], ka = pk4[0], kb4 = pk4[1];
-                    const float pjk[8] = {ja.x * ka.x, ja.y * ka.y, ja.z * ka.z, ja.w * ka.w,
-                                          jb.x * kb4.x, jb.y * kb4.y, jb.z * kb4.z, jb.w * kb4.w};
-                    const float4 *g4 = reinterpret_cast<const float4 *>(ws.grid);
+                {
+                    /* each lane takes a contiguous run of K list entries (K odd, so
+                     * that the lanes' reads of the list fall in distinct banks); the
+                     * list runs row by row, so a lane's entries mostly share j and
+                     * the j-side force is summed in registers and written once per
+                     * change of j */
+                    int K = (hi - lo + 31) >> 5;
+                    if (K > 0) K |= 1;
+                    const int t0 = lo + lane * K;
+                    int cj = -1;
+                    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+                    for (int step = 0; step < K; step++) {
+                        const int t = t0 + step;
+                        if (t >= hi) break;
+                        const unsigned pk = ws.tl[t];
+                        const int jj = pk & 0xffff, kk = pk >> 16;
+                        const float4 d1 = ws.d[jj], d2 = ws.d[kk];
+                        const float wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
+                        const float r3s = wx * wx + wy * wy + wz * wz, r3 = sqrtf(r3s);
+                        if (!(d1.w < drc4 && d2.w < drc4 && r3s < drc4sq)) continue;
+                        float r1 = d1.w, r2 = d2.w, ir1 = ws.ir[jj], ir2 = ws.ir[kk], ir3 = 1.0f / r3;
+                        float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
+                        float f3, df3;
+                        fcutf_d(drc4, r3, f3, df3);
+                        float f1 = ws.fa[jj], df1 = ws.fb[jj], f2 = ws.fa[kk], df2 = ws.fb[kk];
+                        float lz[BNZL], lzp[BNZL];
+                        angularf(P, c, lz, lzp);
+                        float Q = 0.0f, Qe = 0.0f, Qc = 0.0f;
+                        const float4 *pj = reinterpret_cast<const float4 *>(ws.P + jj * 8);
+                        const float4 *pk4 = reinterpret_cast<const float4 *>(ws.P + kk * 8);
+                        const float4 ja = pj[0], jb = pj[1], ka = pk4[0], kb4 = pk4[1];
+                        const float pjk[8] = {ja.x * ka.x, ja.y * ka.y, ja.z * ka.z, ja.w * ka.w,
+                                              jb.x * kb4.x, jb.y * kb4.y, jb.z * kb4.z, jb.w * kb4.w};
+                        const float4 *g4 = reinterpret_cast<const float4 *>(ws.grid);
 #pragma unroll
-                    for (int q = 0; q < BNE; q++) {
-                        const float ex = pjk[q] * expf(-deta[q] * r3s);
-                        const float4 ga = g4[2 * q], gb = g4[2 * q + 1];
-                        const float cg[8] = {ga.x, ga.y, ga.z, ga.w, gb.x, gb.y, gb.z, gb.w};
-                        /* (u, v) = sum over cells of cg * (lz, lz') with paired FMAs */
-                        float2 uv = make_float2(0.0f, 0.0f);
+                        for (int q = 0; q < BNE; q++) {
+                            const float ex = pjk[q] * expf(-deta[q] * r3s);
+                            const float4 ga = g4[2 * q], gb = g4[2 * q + 1];
+                            const float cg[8] = {ga.x, ga.y, ga.z, ga.w, gb.x, gb.y, gb.z, gb.w};
+                            /* (u, v) = sum over cells of cg * (lz, lz') with paired FMAs */
+                            float2 uv = make_float2(0.0f, 0.0f);
 #pragma unroll
-                        for (int zl = 0; zl < BNZL; zl++)
-                            uv = __ffma2_rn(make_float2(cg[zl], cg[zl]), make_float2(lz[zl], lzp[zl]), uv);
-                        const float u = uv.x, vv = uv.y;
-                        Q += ex * u;
-                        Qe += deta[q] * ex * u;
-                        Qc += ex * vv;
-                    }
-                    float Af = 2.0f * f1 * f2 * f3;
-                    float T1 = 2.0f * df1 * f2 * f3 * Q - 2.0f * r1 * Af * Qe;
-                    float T2 = 2.0f * f1 * df2 * f3 * Q - 2.0f * r2 * Af * Qe;
-                    float T3 = 2.0f * f1 * f2 * df3 * Q - 2.0f * r3 * Af * Qe;
-                    float Tc = Af * Qc;
-                    float a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
-                    float a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
-                    g1x = a11 * d1.x + a12 * d2.x - a3 * wx;
-                    g1y = a11 * d1.y + a12 * d2.y - a3 * wy;
-                    g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
-                    g2x = a22 * d2.x + a12 * d1.x + a3 * wx;
-                    g2y = a22 * d2.y + a12 * d1.y + a3 * wy;
-                    g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
-                    }
-                    }
-                    fi0 += g1x + g2x; fi1 += g1y + g2y; fi2 += g1z + g2z;
-                    if (on) {
+                            for (int zl = 0; zl < BNZL; zl++)
+                                uv = __ffma2_rn(make_float2(cg[zl], cg[zl]), make_float2(lz[zl], lzp[zl]), uv);
+                            const float u = uv.x, vv = uv.y;
+                            Q += ex * u;
+                            Qe += deta[q] * ex * u;
+                            Qc += ex * vv;
+                        }
+                        float Af = 2.0f * f1 * f2 * f3;
+                        float T1 = 2.0f * df1 * f2 * f3 * Q - 2.0f * r1 * Af * Qe;
+                        float T2 = 2.0f * f1 * df2 * f3 * Q - 2.0f * r2 * Af * Qe;
+                        float T3 = 2.0f * f1 * f2 * df3 * Q - 2.0f * r3 * Af * Qe;
+                        float Tc = Af * Qc;
+                        float a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
+                        float a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
+                        const float g1x = a11 * d1.x + a12 * d2.x - a3 * wx;
+                        const float g1y = a11 * d1.y + a12 * d2.y - a3 * wy;
+                        const float g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
+                        const float g2x = a22 * d2.x + a12 * d1.x + a3 * wx;
+                        const float g2y = a22 * d2.y + a12 * d1.y + a3 * wy;
+                        const float g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                        fi0 += g1x + g2x; fi1 += g1y + g2y; fi2 += g1z + g2z;
                         atomicAdd(&ws.Fnb[3 * kk], -g2x);
                         atomicAdd(&ws.Fnb[3 * kk + 1], -g2y);
                         atomicAdd(&ws.Fnb[3 * kk + 2], -g2z);
-                    }
-                    /* j side: sum each run of equal j, one atomic per run */
-#pragma unroll
-                    for (int off = 1; off < 32; off <<= 1) {
-                        const float ox = __shfl_down_sync(FULLM, g1x, off), oy = __shfl_down_sync(FULLM, g1y, off),
-                                    oz = __shfl_down_sync(FULLM, g1z, off);
-                        const int ok = __shfl_down_sync(FULLM, jj, off);
-                        if (lane + off < 32 && ok == jj) {
-                            g1x += ox;
-                            g1y += oy;
-                            g1z += oz;
+                        if (jj != cj) {
+                            if (cj >= 0) {
+                                atomicAdd(&ws.Fnb[3 * cj], -sx);
+                                atomicAdd(&ws.Fnb[3 * cj + 1], -sy);
+                                atomicAdd(&ws.Fnb[3 * cj + 2], -sz);
+                            }
+                            cj = jj;
+                            sx = sy = sz = 0.0f;
                         }
+                        sx += g1x; sy += g1y; sz += g1z;
                     }
-                    const int prev = __shfl_up_sync(FULLM, jj, 1);
-                    if (t < hi && (lane == 0 || prev != jj)) {
-                        atomicAdd(&ws.Fnb[3 * jj], -g1x);
-                        atomicAdd(&ws.Fnb[3 * jj + 1], -g1y);
-                        atomicAdd(&ws.Fnb[3 * jj + 2], -g1z);
+                    if (cj >= 0) {
+                        atomicAdd(&ws.Fnb[3 * cj], -sx);
+                        atomicAdd(&ws.Fnb[3 * cj + 1], -sy);
+                        atomicAdd(&ws.Fnb[3 * cj + 2], -sz);
                     }
                 }
                 __syncwarp();
@@ -666,11 +715,16 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
 
 /* ---------------- one evaluation of the structure at DOF vector dof ---------------- */
 
-/* Returns H; gradient into gout; sh.scal[1] = max|F|, sh.scal[2] = max|U-pV|/N. */
-template <int W>
-__device__ double evaluate(const BArgs &A, BShared<W> &sh, const double *dof, double *gout) {
+/* One CTA's share of an evaluation: every atom's position from the DOF
+ * vector, then neighbour lists and the per-atom pass for atoms
+ * rank W + w (mod C W), i.e. warp w of cluster rank `rank`.  Leaves
+ * partial forces in sh.F (all atoms), ea/eu of its own atoms, the per-warp
+ * virials in sh.vir and any overflow in sh.flag. */
+template <int W, int C>
+__device__ void eval_part(const BArgs &A, BShared<W> &sh, const double *dof, int rank) {
     const BParams &P = *A.P;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, N = sh.N, rlxt = A.rlxt;
+    const int first_atom = rank * W + w, stride = C * W;
     float4 *nbd = A.nbd + (size_t)blockIdx.x * BMAXN * BMAXNB;
     int *nbj = A.nbj + (size_t)blockIdx.x * BMAXN * BMAXNB;
     /* structure from the DOF vector (BUF_STR, src/cmin.c:54-88) */
@@ -713,7 +767,7 @@ __device__ double evaluate(const BArgs &A, BShared<W> &sh, const double *dof, do
             shz[t] = c0 * sh.L[2] + c1 * sh.L[5] + c2 * sh.L[8];
             if (c0 == 0 && c1 == 0 && c2 == 0) zero |= 1u << t;
         }
-        for (int i = w; i < N; i += W) {
+        for (int i = first_atom; i < N; i += stride) {
             int count = 0;
             const double xi0 = sh.xc[3 * i], xi1 = sh.xc[3 * i + 1], xi2 = sh.xc[3 * i + 2];
             for (int j = 0; j < N; j++) {
@@ -740,7 +794,7 @@ __device__ double evaluate(const BArgs &A, BShared<W> &sh, const double *dof, do
             }
         }
     } else
-    for (int i = w; i < N; i += W) {
+    for (int i = first_atom; i < N; i += stride) {
         int count = 0;
         const double xi0 = sh.xc[3 * i], xi1 = sh.xc[3 * i + 1], xi2 = sh.xc[3 * i + 2];
         for (int base = 0; base < N * nimg; base += 32) {
@@ -775,10 +829,47 @@ __device__ double evaluate(const BArgs &A, BShared<W> &sh, const double *dof, do
     __syncthreads();
     /* descriptors, MLP and forces, one warp per atom */
     double virw[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = w; i < N; i += W) atom_pass(A, sh, sh.ws[w], i, nbd, nbj, virw);
+    for (int i = first_atom; i < N; i += stride) atom_pass(A, sh, sh.ws[w], i, nbd, nbj, virw);
     if (lane == 0)
         for (int k = 0; k < 6; k++) sh.vir[w][k] = virw[k];
     __syncthreads();
+}
+
+/* Rank 0 of a cluster, after the other ranks' parts are complete: their
+ * partial forces and virials added to its own in rank order, per-atom
+ * energies taken from each atom's owner, overflow flags joined. */
+template <int W, int C>
+__device__ void eval_combine(BShared<W> &sh) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int tid = threadIdx.x, N = sh.N;
+    for (int a = tid; a < N; a += blockDim.x) {
+        const int owner = (a % (C * W)) / W;
+        if (owner != 0) {
+            const BShared<W> *ro = cl.map_shared_rank(&sh, owner);
+            sh.ea[a] = ro->ea[a];
+            sh.eu[a] = ro->eu[a];
+        }
+        for (int q = 0; q < 3; q++) {
+            float f = sh.F[3 * a + q];
+            for (int r = 1; r < C; r++) f += cl.map_shared_rank(&sh, r)->F[3 * a + q];
+            sh.F[3 * a + q] = f;
+        }
+    }
+    for (int k = tid; k < 6 * W; k += blockDim.x) {
+        double v = sh.vir[k / 6][k % 6];
+        for (int r = 1; r < C; r++) v += cl.map_shared_rank(&sh, r)->vir[k / 6][k % 6];
+        sh.vir[k / 6][k % 6] = v;
+    }
+    if (tid == 0)
+        for (int r = 1; r < C; r++) sh.flag |= cl.map_shared_rank(&sh, r)->flag;
+    __syncthreads();
+}
+
+/* FP64 reductions of a complete evaluation (rank 0). */
+template <int W>
+__device__ double eval_finish(const BArgs &A, BShared<W> &sh, double *gout) {
+    const int tid = threadIdx.x, N = sh.N, rlxt = A.rlxt;
     /* FP64 reductions, enthalpy and the DOF gradient (cdfunc_gsl, src/cmin.c:107-166) */
     if (tid == 0) {
         double E = 0.0, U[6];
@@ -839,6 +930,61 @@ __device__ double evaluate(const BArgs &A, BShared<W> &sh, const double *dof, do
     return sh.scal[0];
 }
 
+/* Returns H; gradient into gout; sh.scal[1] = max|F|, sh.scal[2] = max|U-pV|/N.
+ * Called by rank 0 only.  With C > 1 the evaluation is posted to the other
+ * ranks (cluster barrier), every rank evaluates its atoms, and a second
+ * barrier precedes the combination: two barriers per evaluation, matched
+ * one for one by the other ranks' command loop. */
+template <int W, int C>
+__device__ double evaluate(const BArgs &A, BShared<W> &sh, const double *dof, double *gout) {
+    if constexpr (C > 1) {
+        if (threadIdx.x == 0) sh.cmd_dof = dof == sh.x ? 0 : 1;
+        cooperative_groups::this_cluster().sync();
+    }
+    eval_part<W, C>(A, sh, dof, 0);
+    if constexpr (C > 1) {
+        cooperative_groups::this_cluster().sync();
+        eval_combine<W, C>(sh);
+    }
+    return eval_finish<W>(A, sh, gout);
+}
+
+/* Ranks 1..C-1 of a cluster: wait for rank 0's command, copy its DOF
+ * vector, evaluate their atoms, and meet rank 0 at the second barrier.
+ * Rank 0 posts structure -1 when the queue is empty; one last barrier
+ * keeps every rank's shared memory alive until all have read it. */
+template <int W, int C>
+__device__ void cluster_worker(const BArgs &A, BShared<W> &sh, int rank) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int tid = threadIdx.x;
+    int cur = -1;
+    for (;;) {
+        cl.sync();
+        const BShared<W> *r0 = cl.map_shared_rank(&sh, 0);
+        const int s = r0->cmd_s, which = r0->cmd_dof;
+        if (s < 0) break;
+        const int N = A.nat[s], o = A.off[s];
+        const int n = 3 * N + (A.rlxt == 3 ? 9 : 0);
+        if (s != cur) {
+            if (tid == 0) {
+                sh.N = N;
+                sh.ndof = n;
+                sh.flag = 0;
+                for (int k = 0; k < 9; k++) sh.L[k] = A.lat[9 * s + k];
+            }
+            for (int a = tid; a < N; a += blockDim.x) sh.spc[a] = A.spc[o + a];
+            cur = s;
+        }
+        const double *src = which ? r0->xt : r0->x;
+        for (int k = tid; k < n; k += blockDim.x) sh.x[k] = src[k];
+        __syncthreads();
+        eval_part<W, C>(A, sh, sh.x, rank);
+        cl.sync();
+    }
+    cl.sync();
+}
+
 /* cubic (or quadratic without db) minimiser on [lo,hi] (Fletcher, sec. 2.6) */
 __device__ double interp_min(double a, double fa, double da, double b, double fb, double db, double lo, double hi) {
     double w = b - a;
@@ -876,11 +1022,18 @@ __device__ void vcopy(double *dst, const double *src, int n) {
     for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
 }
 
-template <int W>
+template <int W, int C>
 __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
     extern __shared__ __align__(16) char smem_raw[];
     BShared<W> &sh = *reinterpret_cast<BShared<W> *>(smem_raw);
     const int tid = threadIdx.x;
+    if constexpr (C > 1) {
+        const int rank = (int)cooperative_groups::this_cluster().block_rank();
+        if (rank != 0) {
+            cluster_worker<W, C>(A, sh, rank);
+            return;
+        }
+    }
     double *H = A.hmat + (size_t)blockIdx.x * BMAXDOF * BMAXDOF;
     const double rho = 0.01, tau1 = 9.0, tau2 = 0.05, tau3 = 0.5;
     for (;;) {
@@ -891,6 +1044,7 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
         const int N = A.nat[s], o = A.off[s], rlxt = A.rlxt;
         const int n = 3 * N + (rlxt == 3 ? 9 : 0);
         if (tid == 0) {
+            sh.cmd_s = s;
             sh.N = N;
             sh.ndof = n;
             sh.flag = 0;
@@ -913,7 +1067,7 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
         }
         for (int k = tid; k < n * n; k += blockDim.x) H[k] = (k / n == k % n) ? 1.0 : 0.0;
         __syncthreads();
-        double f = evaluate(A, sh, sh.x, sh.g), fprev = f;
+        double f = evaluate<W, C>(A, sh, sh.x, sh.g), fprev = f;
         double maxf = sh.scal[1], maxu = sh.scal[2];
         int first = 1, iter = 0, status = 1;
         if (sh.flag) status = 2;
@@ -957,7 +1111,7 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
             for (trial = 0; trial < 60 && !done; trial++) {
                 for (int k = tid; k < n; k += blockDim.x) sh.xt[k] = sh.x[k] + alpha * sh.p[k];
                 __syncthreads();
-                ft = evaluate(A, sh, sh.xt, sh.gt);
+                ft = evaluate<W, C>(A, sh, sh.xt, sh.gt);
                 double t = 0.0;
                 for (int k = tid; k < n; k += blockDim.x) t += sh.gt[k] * sh.p[k];
                 dt = cta_sum(sh, t);
@@ -1094,6 +1248,12 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
                 A.x[3 * (size_t)(o + a) + q] = sh.x[3 * a] * sh.L[q] + sh.x[3 * a + 1] * sh.L[3 + q] + sh.x[3 * a + 2] * sh.L[6 + q];
         __syncthreads();
     }
+    if constexpr (C > 1) {
+        /* queue empty: the exit command, then the last barrier */
+        if (tid == 0) sh.cmd_s = -1;
+        cooperative_groups::this_cluster().sync();
+        cooperative_groups::this_cluster().sync();
+    }
 }
 
 }  // namespace
@@ -1146,13 +1306,50 @@ static int build_bparams(const mb_model *m, BParams *B, float **w_out, size_t *w
     return 0;
 }
 
-/* launch geometry of k_relax_batch<W> on this device */
-template <int W>
-static cudaError_t batch_config(int *per) {
+/* launch geometry of k_relax_batch<W, C> on this device: how many CTAs
+ * (C = 1) or clusters of C CTAs can be resident at once */
+static void cluster_config(cudaLaunchConfig_t *cfg, cudaLaunchAttribute *at, int units, int W, int C, size_t smem,
+                           cudaStream_t st) {
+    *cfg = cudaLaunchConfig_t{};
+    cfg->gridDim = dim3(units * C);
+    cfg->blockDim = dim3(W * 32);
+    cfg->dynamicSmemBytes = smem;
+    cfg->stream = st;
+    at->id = cudaLaunchAttributeClusterDimension;
+    at->val.clusterDim.x = C;
+    at->val.clusterDim.y = 1;
+    at->val.clusterDim.z = 1;
+    cfg->attrs = at;
+    cfg->numAttrs = 1;
+}
+
+template <int W, int C>
+static cudaError_t batch_config(int sms, int *units) {
     const size_t smem = sizeof(BShared<W>);
-    cudaError_t e = cudaFuncSetAttribute(k_relax_batch<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_relax_batch<W, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, k_relax_batch<W>, W * 32, smem);
+    if (C == 1) {
+        int per = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_batch<W, C>, W * 32, smem);
+        *units = per * sms;
+        return e;
+    }
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute at;
+    cluster_config(&cfg, &at, 1, W, C, smem, 0);
+    return cudaOccupancyMaxActiveClusters(units, k_relax_batch<W, C>, &cfg);
+}
+
+template <int W, int C>
+static cudaError_t batch_launch(int units, cudaStream_t st, const BArgs &a) {
+    if (C == 1) {
+        k_relax_batch<W, C><<<units, W * 32, sizeof(BShared<W>), st>>>(a);
+        return cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute at;
+    cluster_config(&cfg, &at, units, W, C, sizeof(BShared<W>), st);
+    return cudaLaunchKernelEx(&cfg, k_relax_batch<W, C>, a);
 }
 
 extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const int *d_off, const int *d_spc,
@@ -1164,19 +1361,32 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
     float *hw = nullptr;
     size_t wlen = 0;
     if (build_bparams(m, &hp, &hw, &wlen)) return (int)cudaErrorInvalidValue;
-    int dev = 0, sms = 0, per = 0;
+    int dev = 0, sms = 0, units = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int wide = 1;
+    /* A population that fits the SMs in about two rounds is bound by its
+     * slowest BFGS chains: clusters of 4 CTAs (4 SMs) evaluate each structure,
+     * cutting a chain's latency about threefold (256 Mg-Ca structures: 0.88 s
+     * against 1.60 s).  Larger populations keep one CTA per structure, which
+     * has the higher throughput (4096 Cu-Pd-Ag offspring: 2.10 s against
+     * 2.48 s with pairs). */
+    int wide = 1, csize = S <= 2 * sms ? 4 : 1;
     {
-        /* MAISE_B200_BATCH_WARPS=4 selects the narrow CTA (A/B timing) */
-        const char *fw = getenv("MAISE_B200_BATCH_WARPS");
+        /* MAISE_B200_BATCH_WARPS=4 selects the narrow CTA and
+         * MAISE_B200_BATCH_CLUSTER=1|2|4 the CTAs per structure (A/B timing) */
+        const char *fw = getenv("MAISE_B200_BATCH_WARPS"), *fc = getenv("MAISE_B200_BATCH_CLUSTER");
         if (fw) wide = atoi(fw) != 4;
+        if (fc) csize = atoi(fc) == 4 ? 4 : atoi(fc) == 2 ? 2 : 1;
+        if (!wide) csize = 1;
     }
-    cudaError_t e = wide ? batch_config<BWARPS_WIDE>(&per) : batch_config<4>(&per);
+    cudaError_t e = !wide        ? batch_config<4, 1>(sms, &units)
+                    : csize == 4 ? batch_config<BWARPS_WIDE, 4>(sms, &units)
+                    : csize == 2 ? batch_config<BWARPS_WIDE, 2>(sms, &units)
+                                 : batch_config<BWARPS_WIDE, 1>(sms, &units);
     if (e != cudaSuccess) { free(hw); return (int)e; }
-    if (per < 1) { free(hw); return (int)cudaErrorInvalidConfiguration; }
-    int grid = sms * per < S ? sms * per : S;
+    if (units < 1) { free(hw); return (int)cudaErrorInvalidConfiguration; }
+    const int gunits = units < S ? units : S; /* CTAs, or clusters of csize CTAs */
+    const int grid = gunits * csize;
     BParams *dp = nullptr;
     float *dw = nullptr;
     double *hm = nullptr;
@@ -1205,12 +1415,12 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
         a.lat = d_lat; a.x = d_x; a.H = d_H; a.iters = d_iters; a.status = d_status;
         a.P = dp; a.W = dw; a.queue = queue; a.hmat = hm; a.nbd = nbd; a.nbj = nbj; a.evals = evals;
         cudaEventRecord(e0, st);
-        if (wide)
-            k_relax_batch<BWARPS_WIDE><<<grid, BWARPS_WIDE * 32, sizeof(BShared<BWARPS_WIDE>), st>>>(a);
-        else
-            k_relax_batch<4><<<grid, 4 * 32, sizeof(BShared<4>), st>>>(a);
+        e = !wide        ? batch_launch<4, 1>(gunits, st, a)
+            : csize == 4 ? batch_launch<BWARPS_WIDE, 4>(gunits, st, a)
+            : csize == 2 ? batch_launch<BWARPS_WIDE, 2>(gunits, st, a)
+                         : batch_launch<BWARPS_WIDE, 1>(gunits, st, a);
         cudaEventRecord(e1, st);
-        e = cudaGetLastError();
+        if (!e) e = cudaGetLastError();
     }
     if (!e) e = cudaStreamSynchronize(st);
     if (!e && evals_out) e = cudaMemcpy(evals_out, evals, sizeof(long long), cudaMemcpyDeviceToHost);

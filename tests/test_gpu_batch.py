@@ -30,18 +30,23 @@ def _nat(pop):
     return np.array([len(s["atmn"]) for s in pop])
 
 
-@pytest.fixture(params=["12", "4"], ids=["12warps", "4warps"])
+@pytest.fixture(params=[("12", "1"), ("4", "1"), ("12", "2"), ("12", "4")],
+                ids=["12warps", "4warps", "12warps-cluster2", "12warps-cluster4"])
 def width(request, monkeypatch):
-    """Warps per structure of the batched kernel (the library reads
-    MAISE_B200_BATCH_WARPS at every launch; 12 is the default)."""
-    monkeypatch.setenv("MAISE_B200_BATCH_WARPS", request.param)
-    return int(request.param)
+    """Warps per CTA and CTAs per structure (a thread-block cluster sharing
+    the structure's evaluations) of the batched kernel.  The library reads
+    MAISE_B200_BATCH_WARPS and MAISE_B200_BATCH_CLUSTER at every launch; by
+    default it uses 12 warps, with clusters of 4 for populations of at most
+    two structures per SM."""
+    monkeypatch.setenv("MAISE_B200_BATCH_WARPS", request.param[0])
+    monkeypatch.setenv("MAISE_B200_BATCH_CLUSTER", request.param[1])
+    return request.param
 
 
 def test_fp32_energy_of_start_structures_matches_fp64(mgca, width):
     """With no iterations the batched path reports each structure's enthalpy
-    from its FP32 evaluation: within 1e-5 eV/atom of the FP64 path, with
-    either CTA width."""
+    from its FP32 evaluation: within 1e-5 eV/atom of the FP64 path, for
+    every CTA width and cluster size."""
     pot, pop = mgca
     r = pot.relax_batch(pop, urep=UREP, rlxt=3, mitr=0, fmax=FMAX)
     for k, s in enumerate(pop):

@@ -1383,6 +1383,13 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
                     : csize == 4 ? batch_config<BWARPS_WIDE, 4>(sms, &units)
                     : csize == 2 ? batch_config<BWARPS_WIDE, 2>(sms, &units)
                                  : batch_config<BWARPS_WIDE, 1>(sms, &units);
+    if (csize > 1 && (e != cudaSuccess || units < 1)) {
+        /* clusters of this size cannot be placed (e.g. on a partitioned
+         * GPU): one CTA per structure */
+        cudaGetLastError();
+        csize = 1;
+        e = batch_config<BWARPS_WIDE, 1>(sms, &units);
+    }
     if (e != cudaSuccess) { free(hw); return (int)e; }
     if (units < 1) { free(hw); return (int)cudaErrorInvalidConfiguration; }
     const int gunits = units < S ? units : S; /* CTAs, or clusters of csize CTAs */

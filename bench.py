@@ -39,6 +39,8 @@ METRIC = "atom-steps/s (E+F+stress) & relaxed structures/s vs plain GPU path"
 UNIT = "atom-steps/s"
 WORKLOAD = "CuPdAg fcc 10x10x10 (4000 atoms), 282-10-10-1 FP64, Rc 6 A, NVT 600 K, dt 1 fs"
 SETTLE_STEPS = 20  # untimed NVT steps from the ideal lattice before the warm-up
+KERNEL_NAME = ("descriptor pass: k_legs (leg tables) + k_efs_leg (fused descriptors + MLP + forces + virial), "
+               "timed together")
 
 
 def workload(seed=0):
@@ -172,7 +174,8 @@ def cpu_baseline(w, model_dir, max_seconds=40.0):
         times.append(time.perf_counter() - t0)
     per = float(np.median(times))
     return {"value": len(at) / per, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"{len(times)} CALL_MAISE E+F+S calls on the 4000-atom structure (first call, "
+            "sample": f"{len(times)} CALL_MAISE E+F+S calls on the 4000-atom structure at the end of the timed "
+                      f"MD (first call, "
                       f"{t_first:.1f} s incl. allocation, excluded); median {per:.3f} s per call"}
 
 
@@ -195,11 +198,12 @@ def _binding_model(td, name, structures, spcz, seed, angular=0.3):
     return os.path.join(path, "model")
 
 
-def population_relax(local, td, plain_sample=16, mitr=1000, fmax=0.01, urep=100.0):
+def population_relax(local, td, plain_sample=64, mitr=1000, fmax=0.01, urep=100.0):
     """Relaxed structures/s of the persistent batched relax (FP32 descriptors
     and MLP, FP64 reductions and BFGS) against the plain one-structure FP64
-    path (host BFGS over the GPU E/F/S) on a sample of the same population;
-    every batched minimum is re-evaluated by the FP64 path."""
+    path (host BFGS over the GPU E/F/S) on a seeded random sample of 64
+    structures of the same population; every batched minimum is
+    re-evaluated by the FP64 path."""
     import maise_b200
     from maise_b200 import workloads
 
@@ -217,9 +221,10 @@ def population_relax(local, td, plain_sample=16, mitr=1000, fmax=0.01, urep=100.
         f64.append(float(np.abs(r["F"]).max()))
     dE, f64 = np.array(dE), np.array(f64)
     conv = rb["status"] == 0
+    sample = np.sort(np.random.default_rng(17).choice(len(pop), plain_sample, replace=False))
     t0 = time.perf_counter()
-    plain = [pot.relax_fmax(s["X"], s["LAT"], s["atmn"], ND=3, NM=300, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
-             for s in pop[:plain_sample]]
+    plain = [pot.relax_fmax(pop[k]["X"], pop[k]["LAT"], pop[k]["atmn"], ND=3, NM=300, urep=urep, rlxt=3, mitr=mitr,
+                            fmax=fmax) for k in sample]
     t_plain = time.perf_counter() - t0
     batched = len(pop) / (rb["ms"] / 1e3)
     plain_sps = plain_sample / t_plain
@@ -227,7 +232,9 @@ def population_relax(local, td, plain_sample=16, mitr=1000, fmax=0.01, urep=100.
     return {"workload": POP_WORKLOAD, "structures": len(pop), "atoms": int(nat.sum()),
             "batched_structures_per_s": batched, "batched_e2e_structures_per_s": len(pop) / wall,
             "plain_structures_per_s": plain_sps, "speedup_vs_plain": batched / plain_sps,
-            "plain_sample": f"first {plain_sample} structures of the population, one mb_relax_fmax each",
+            "plain_sample": f"{plain_sample} structures drawn at random (seed 17) from the population, one "
+                            f"mb_relax_fmax each; their atom counts average {nat[sample].mean():.1f} against "
+                            f"{nat.mean():.1f} for all",
             "batched_converged": int(conv.sum()), "plain_converged": int(sum(r["converged"] for r in plain)),
             "batched_evals": rb["evals"], "kernel_ms": rb["ms"],
             "fp32_vs_fp64_ev_per_atom_max_converged": float(dE[conv].max()) if conv.any() else None,
@@ -235,8 +242,32 @@ def population_relax(local, td, plain_sample=16, mitr=1000, fmax=0.01, urep=100.
             "dtype": "descriptors/MLP fp32, reductions/BFGS fp64"}
 
 
+def plain_relax_many(model, structures, device, urep, mitr, fmax, threads=8):
+    """Relaxed enthalpies of `structures` by the plain FP64 path (mb_relax_fmax),
+    one handle per host thread so that independent relaxations overlap on
+    the GPU (the handle API is per thread)."""
+    import concurrent.futures as cf
+
+    import maise_b200
+
+    chunks = [list(range(k, len(structures), threads)) for k in range(threads)]
+    H = np.zeros(len(structures))
+
+    def run(idx):
+        pot = maise_b200.Potential(model, device=device)
+        for k in idx:
+            s = structures[k]
+            H[k] = pot.relax_fmax(s["X"], s["LAT"], s["atmn"], ND=3, NM=300, urep=urep, rlxt=3, mitr=mitr,
+                                  fmax=fmax)["H"]
+        pot.close()
+
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(run, chunks))
+    return H
+
+
 def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs=60, mitr=300, fmax=0.01,
-                         urep=100.0):
+                         urep=100.0, plain_judge=256):
     """One EA generation with and without the surrogate screen: relax every
     offspring, or predict all, keep the best quarter and relax those; the
     full relaxation of every offspring judges the screen's recall of the
@@ -248,7 +279,8 @@ def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs
     spc = (29, 46, 47)
     train = workloads.ea_population_chunked(n_train, seed=11, nmin=16, nmax=48, species=spc)
     gen = workloads.ea_population_chunked(n_gen, seed=12, nmin=16, nmax=48, species=spc)
-    pot = maise_b200.Potential(_binding_model(td, "gen", train, spc, 5), device=local)
+    model_gen = _binding_model(td, "gen", train, spc, 5)
+    pot = maise_b200.Potential(model_gen, device=local)
     t0 = time.perf_counter()
     rt = pot.relax_batch(train, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
     t_data = time.perf_counter() - t0
@@ -270,15 +302,162 @@ def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs
     rk = pot.relax_batch([gen[i] for i in kept], urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
     t_scr = time.perf_counter() - t0
     e0 = np.array([pot.energy(s["X"], s["LAT"], s["atmn"], ND=3, NM=300, urep=urep)["H"] for s in gen]) / nat
+    # composition alone: least squares of the training labels on the species fractions
+    def frac(ss):
+        return np.array([[np.mean(np.asarray(s["atmn"]) == k) for k in range(len(spc))] + [1.0] for s in ss])
+
+    coef, *_ = np.linalg.lstsq(frac(train), y, rcond=None)
+    pcomp = frac(gen) @ coef
+    # the plain FP64 relax (host BFGS over the GPU E+F+S, one structure at a
+    # time per handle, 8 handles on host threads) of a random sample judges
+    # the screen on that sample
+    sample = np.sort(np.random.default_rng(23).choice(n_gen, plain_judge, replace=False))
+    t0 = time.perf_counter()
+    plain = plain_relax_many(model_gen, [gen[k] for k in sample], local, urep=urep, mitr=mitr, fmax=fmax)
+    t_plain = time.perf_counter() - t0
+    truth_plain = plain / nat[sample]
+    in_kept = np.zeros(n_gen, bool)
+    in_kept[kept] = True
+    ntop = max(1, int(round(0.10 * len(sample))))
+    top = np.argsort(truth_plain, kind="stable")[:ntop]
+    recall_plain = float(in_kept[sample[top]].mean())
     sur.close()
     pot.close()
     return {"workload": GEN_WORKLOAD, "offspring": n_gen, "train_pairs": n_train, "keep": keep,
             "recall_top10": recall(pred, truth, keep), "recall_top10_by_unrelaxed_energy": recall(e0, truth, keep),
+            "recall_top10_by_composition": recall(pcomp, truth, keep),
+            "mae_ev_per_atom": {"surrogate": float(np.abs(pred - truth).mean()),
+                                "composition": float(np.abs(pcomp - truth).mean())},
+            "recall_top10_plain_judged": recall_plain,
+            "plain_judge_sample": f"{len(sample)} offspring drawn at random (seed 23), each relaxed by the plain FP64 "
+                                  f"path (mb_relax_fmax) in {t_plain:.1f} s; recall = share of the sample's best "
+                                  f"{ntop} that the screen keeps",
+            "plain_vs_batched_ev_per_atom_median": float(np.median(np.abs(truth_plain - truth[sample]))),
             "recall_top10_random_expectation": keep,
             "generation_s_relax_all": t_all, "generation_s_screened": t_scr, "speedup": t_all / t_scr,
             "screen_s": t_pred, "relax_all_kernel_ms": ra["ms"], "relax_kept_kernel_ms": rk["ms"],
             "train_data_relax_s": t_data, "fit_s": t_fit, "epochs": epochs, "final_loss": float(loss[-1]),
             "judge": "batched relax of every offspring (FP32 descriptors/MLP, FP64 BFGS)"}
+
+
+def _efs_rate(pot, w, ND, calls, NM):
+    """atom-steps/s of E+F+S through mb_efs (host arrays in and out), plus
+    the fused kernel's time and pair/triplet counts over those calls."""
+    pot.efs(w["X"], w["LAT"], w["atmn"], ND=ND, NM=NM)  # tuning, capacity, graph capture
+    pot.efs(w["X"], w["LAT"], w["atmn"], ND=ND, NM=NM)
+    pot.profile(True, capacity=calls + 4)
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        pot.efs(w["X"], w["LAT"], w["atmn"], ND=ND, NM=NM)
+    dt = time.perf_counter() - t0
+    k = pot.profile_read()
+    pot.profile(False)
+    return len(w["atmn"]) * calls / dt, k
+
+
+def _roofline(basis, nspc, k, N, peak):
+    n = max(1, k["launches"])
+    ms = k["ms_total"] / n
+    fl = algorithmic_flops(basis, nspc, k["pairs"] / n, k["triplets"] / n, N)
+    ach = fl / (ms * 1e-3) / 1e12
+    return {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+            "kernel": KERNEL_NAME, "ms_per_launch": ms, "flops_per_launch": fl,
+            "pairs_per_atom": k["pairs"] / n / N, "triplets_per_atom": k["triplets"] / n / N}
+
+
+CFG1_WORKLOAD = ("Cu fcc 2x2x2 conventional (32 atoms, a = 3.61 A, Gaussian 0.05 A jitter), 51-10-10-1 tanh FP64, "
+                 "Rc 6 A: E+F+S, then a 200-iteration BFGS cell relax (RLXT 3)")
+CFG4_WORKLOAD = ("Au fcc particle (a = 4.08 A, 5% vacancies, 0.05 A jitter, 15 A vacuum padding, no periodic "
+                 "directions), 51-10-10-1 tanh FP64, Rc 6 A: E+F+S, then 500 NVT steps at 300 K")
+
+
+def config1_leg(local, td, peak, cpu=True):
+    """The small plain-method case: E+F+S atom-steps/s and a 200-iteration
+    BFGS relax (structures/s) through the C-ABI, against the reference
+    sources (CALL_MAISE and CELL_RELX over the project BFGS) on the host
+    cores in the same run."""
+    import maise_b200
+    from maise_b200 import models, workloads
+
+    w = workloads.fcc_supercell(n=2, a=3.61, jitter=0.05, seed=0)
+    d = os.path.join(td, "cfg1")
+    os.makedirs(d, exist_ok=True)
+    basis = models.Basis()
+    models.random_model(os.path.join(d, "model"), w["spcz"], basis, (w["X"], w["LAT"], w["atmn"], 3), seed=1)
+    pot = maise_b200.Potential(os.path.join(d, "model"), device=local)
+    rate, k = _efs_rate(pot, w, 3, 2000, 200)
+    pot.relax(w["X"], w["LAT"], w["atmn"], ND=3, NM=200, rlxt=3, mitr=5, etol=0.0)  # warm-up
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        r = pot.relax(w["X"], w["LAT"], w["atmn"], ND=3, NM=200, rlxt=3, mitr=200, etol=0.0)
+    t_relax = (time.perf_counter() - t0) / reps
+    out = {"workload": CFG1_WORKLOAD, "atoms": 32, "efs_atom_steps_per_s": rate,
+           "roofline": _roofline(basis, 1, k, 32, peak), "relax_structures_per_s": 1.0 / t_relax,
+           "relax_iterations": r["iters"], "relax_H": r["H"], "relax_calls": [r["n_energy"], r["n_force"]]}
+    pot.close()
+    if cpu:
+        from oracle import RefOracle, ref_available
+
+        if ref_available():
+            cores = os.cpu_count() or 1
+            ref = RefOracle(d, cores)
+            ref.efs(w["X"], w["LAT"], w["atmn"], 3, NM=200)
+            n, t0 = 0, time.perf_counter()
+            while n < 20 or time.perf_counter() - t0 < 2.0:
+                ref.efs(w["X"], w["LAT"], w["atmn"], 3, NM=200)
+                n += 1
+            ref_rate = 32 * n / (time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            rr = ref.relax(w["X"], w["LAT"], w["atmn"], 3, rlxt=3, mitr=200, etol=0.0, NM=200)
+            t_ref = time.perf_counter() - t0
+            out["cpu_baseline"] = {"efs_atom_steps_per_s": ref_rate, "relax_structures_per_s": 1.0 / t_ref,
+                                   "relax_iterations": rr["iters"], "relax_H": rr["H"], "cores": cores,
+                                   "kind": "reference",
+                                   "sample": f"{n} CALL_MAISE calls; one CELL_RELX of up to 200 iterations"}
+    return out
+
+
+def particle_leg(local, td, peak, md_steps=500, cpu=True):
+    """The large cluster: E+F+S atom-steps/s through mb_efs and 500 NVT steps
+    at 300 K on the device (mb_md_nvt), against one reference CALL_MAISE on
+    the host cores (first call, which allocates, excluded)."""
+    import maise_b200
+    from maise_b200 import atomic_mass, maxwell, models, workloads
+
+    w = workloads.fcc_particle()
+    N = len(w["atmn"])
+    d = os.path.join(td, "cfg4")
+    os.makedirs(d, exist_ok=True)
+    basis = models.Basis()
+    models.random_model(os.path.join(d, "model"), w["spcz"], basis, (w["X"], w["LAT"], w["atmn"], 0), seed=1)
+    pot = maise_b200.Potential(os.path.join(d, "model"), device=local)
+    rate, k = _efs_rate(pot, w, 0, 50, 100)
+    V0 = maxwell([atomic_mass(w["spcz"][s]) for s in w["atmn"]], 300.0, seed=7)
+    st = pot.md_nvt(w["X"], w["LAT"], w["atmn"], V0, 300.0, nsteps=10, ND=0, NM=100, trace=False)  # warm-up
+    pot.md_profile(True, capacity=md_steps + 16)
+    st = pot.md_nvt(st["X"], w["LAT"], w["atmn"], st["V"], 300.0, nsteps=md_steps, ND=0, NM=100, xi=st["xi"],
+                    trace=True)
+    md = pot.md_profile_read()
+    pot.md_profile(False)
+    out = {"workload": CFG4_WORKLOAD, "atoms": N, "efs_atom_steps_per_s": rate,
+           "roofline": _roofline(basis, 1, k, N, peak),
+           "md_atom_steps_per_s": N * md["steps"] / (md["ms_total"] / 1e3), "md_steps": md["steps"],
+           "md_final_K_eV": float(st["K"][-1])}
+    pot.close()
+    if cpu:
+        from oracle import RefOracle, ref_available
+
+        if ref_available():
+            cores = os.cpu_count() or 1
+            ref = RefOracle(d, cores)
+            ref.efs(w["X"], w["LAT"], w["atmn"], 0, NM=100)
+            t0 = time.perf_counter()
+            ref.efs(w["X"], w["LAT"], w["atmn"], 0, NM=100)
+            t_ref = time.perf_counter() - t0
+            out["cpu_baseline"] = {"efs_atom_steps_per_s": N / t_ref, "cores": cores, "kind": "reference",
+                                   "sample": "one CALL_MAISE E+F+S of the whole particle (first call excluded)"}
+    return out
 
 
 def profile_case(case):
@@ -311,8 +490,23 @@ def profile_case(case):
         sur.screen(pop)
 
 
+def bench_config(N, world):
+    """The `config` of both arms' lines (they run the same protocol)."""
+    return {"workload": WORKLOAD, "atoms": N, "parallelism": f"replicas x{world}", "settle_steps": SETTLE_STEPS,
+            "l2": "256 MiB buffer overwritten between timed steps (outside the step events)",
+            "model": "random N(0,1/fan_in) weights, input ranges from the structure"}
+
+
+REF_MAX_STEPS = 60  # longest timed run of the reference arm (about 4.4 s per step on 16 cores)
+
+
 def run_reference(args, rank, world):
-    """--impl reference: the reference CPU implementation on the same workload."""
+    """--impl reference: the reference MAISE sources (oracle/_ref, compiled from
+    the reference's own files) run the same protocol as the GPU arm on the
+    host cores -- the reference's Maxwell velocities (seed 7), SETTLE_STEPS
+    untimed NVT steps, W untimed warm-up steps, then K timed steps of
+    CELL_FRC + the NVT update of Dynamics (src/cmod.c:403-453).  Nothing of
+    libmaise_b200 is loaded.  Ranks other than 0 exit without work."""
     from oracle import RefOracle, ref_available
 
     if rank != 0:
@@ -321,32 +515,25 @@ def run_reference(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "reference sources were not compiled (oracle/_ref)"}))
         return
     w, basis = workload()
+    N = len(w["atmn"])
     cores = os.cpu_count() or 1
+    steps = min(args.steps, REF_MAX_STEPS)
     with tempfile.TemporaryDirectory() as td:
         make_model(td, w, basis)
         ref = RefOracle(td, cores)
-        from maise_b200 import atomic_mass, maxwell
-
-        V = maxwell([atomic_mass(w["spcz"][s]) for s in w["atmn"]], 600.0, seed=7)
+        V = ref.maxwell(w["X"], w["LAT"], w["atmn"], 3, 600.0, seed=7, NM=100)
+        st = ref.nvt(w["X"], w["LAT"], w["atmn"], 3, 600.0, 1.0, 25.0, SETTLE_STEPS + args.warmup, V=V, NM=100)
         t0 = time.perf_counter()
-        ref.nvt(w["X"], w["LAT"], w["atmn"], 3, 600.0, 1.0, 25.0, max(1, min(args.warmup, 1)), V=V, NM=100)
-        t_warm = time.perf_counter() - t0
-        steps = args.steps
-        per_est = t_warm / max(1, min(args.warmup, 1))
-        budget = 150.0
-        if per_est * steps > budget:
-            steps = max(1, int(budget / per_est))
-        t0 = time.perf_counter()
-        ref.nvt(w["X"], w["LAT"], w["atmn"], 3, 600.0, 1.0, 25.0, steps, V=V, NM=100)
+        st = ref.nvt(st["X"], w["LAT"], w["atmn"], 3, 600.0, 1.0, 25.0, steps, V=st["V"], xi=st["xi"], NM=100)
         dt = time.perf_counter() - t0
-    value = len(w["atmn"]) * steps / dt
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    value = N * steps / dt
+    sample = (f"{steps} timed NVT steps of the 4000-atom structure (CELL_FRC + NVT update, OpenMP) after "
+              f"{SETTLE_STEPS} settle and {args.warmup} warm-up steps from the reference's Maxwell velocities")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "impl": "reference MAISE sources, CELL_FRC + NVT step, OpenMP"},
-            "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"{steps} NVT steps of the 4000-atom structure (first CALL_MAISE excluded)"},
+            "config": bench_config(N, world), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -360,6 +547,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-population", action="store_true", help="skip the population relax and surrogate legs")
+    ap.add_argument("--no-extra-legs", action="store_true", help="skip the 32-atom cell and 20000-atom particle legs")
     ap.add_argument("--profile-case", choices=["md", "relax-batch", "surrogate"],
                     help="run one small case of a hot kernel for an ncu capture and exit (no bench line)")
     args = ap.parse_args()
@@ -465,7 +653,7 @@ def main():
     achieved = flops / (ms_k * 1e-3) / 1e12
     roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
             "frac": achieved / fp64_peak, "traffic": profile_traffic(),
-            "kernel": "k_efs (fused descriptors + MLP + forces + virial)", "ms_per_launch": ms_k,
+            "kernel": KERNEL_NAME, "ms_per_launch": ms_k,
             "flops_per_launch": flops, "pairs_per_atom": kern["pairs"] / launches_k / N,
             "triplets_per_atom": kern["triplets"] / launches_k / N,
             "peak_source": "FP64 FMA-chain probe measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
@@ -474,10 +662,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * step_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "atoms": N, "parallelism": f"replicas x{world}",
-                       "settle_steps": SETTLE_STEPS,
-                       "l2": "256 MiB buffer overwritten between timed steps (outside the step events)",
-                       "model": "random N(0,1/fan_in) weights, input ranges from the structure"},
+            "config": bench_config(N, world),
             "e2e": e2e, "roofline": roof, "gpu_launches": launches, "clocks": clocks}
     def leg(name, fn):
         t0 = time.perf_counter()
@@ -486,10 +671,14 @@ def main():
         return r
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = leg("cpu_baseline", lambda: cpu_baseline(w, td))
+        line["cpu_baseline"] = leg("cpu_baseline", lambda: cpu_baseline(dict(w, X=st["X"]), td))
     if rank == 0 and not args.no_population:
         line["population_relax"] = leg("population_relax", lambda: population_relax(local, td))
         line["surrogate_generation"] = leg("surrogate_generation", lambda: surrogate_generation(local, td))
+    if rank == 0 and not args.no_extra_legs:
+        cpu = world == 1 and not args.no_cpu_baseline
+        line["small_cell"] = leg("small_cell", lambda: config1_leg(local, td, fp64_peak, cpu=cpu))
+        line["particle"] = leg("particle", lambda: particle_leg(local, td, fp64_peak, cpu=cpu))
     if rank == 0:
         print(json.dumps(line))
         print(f"[bench] total: {time.perf_counter() - t_start:.1f} s", file=sys.stderr, flush=True)

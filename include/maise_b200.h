@@ -87,6 +87,20 @@ int mb_descriptors(mb_potential *pot, int N, int NM, int ND, int XT, const int *
 int mb_descriptor_vjp(mb_potential *pot, int N, int NM, int ND, int XT, const int *atmn, const double *lat9,
                       const double *x, const double *g, double *frc, double *str);
 
+/* The neighbour list the E/F/S passes build (LIST, src/cell.c:82-185): for
+ * every atom i each (atom j, lattice image) with |x_j + S - x_i|^2 < Rc^2
+ * (strict), S = sum_q shift_q L_q, excluding i's own zero image, after the
+ * wrap into the cell that LIST performs.  The set is the reference's; the
+ * order within an atom's list is not (LIST swaps the nearest into slot 0).
+ *   path   0 as the passes choose, 1 the all-pairs search, 2 the cell list
+ *          (MB_ERR_ARG if a periodic direction is under 3 Rc wide)
+ *   cap    row length of nj and shift
+ * Outputs: nn[N] counts, nj[N*cap] neighbour atoms, shift[N*cap*3] integer
+ * images, x_wrapped[3N] (may be NULL).  MB_ERR_CAPACITY if an atom has more
+ * than cap neighbours; MB_ERR_NEIGHBOURS if one reaches NM. */
+int mb_neighbours(mb_potential *pot, int N, int NM, int ND, int XT, const int *atmn, const double *lat9,
+                  const double *x, int path, int cap, int *nn, int *nj, int *shift, double *x_wrapped);
+
 /* Cell relaxation (CELL_RELX/CELL_MIN, src/cmod.c:901-977,
  * src/cmin.c:22-301).  Degrees of freedom as STR_BUF: fractional atom
  * coordinates (rlxt 2), plus the 9 lattice components (rlxt 3), or the
@@ -118,6 +132,73 @@ int mb_relax_fmax(mb_potential *pot, int N, int NM, int ND, const int *atmn, dou
  * 2 (too many neighbours), 3 (no descent possible). */
 int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, double *lat, double *x, double p_gpa,
                    double urep, int rlxt, int mitr, double fmax, double *H, int *iters, int *status);
+
+/* Energy, forces and virial of every structure of a population, computed
+ * by the evaluation of mb_relax_batch (FP32 descriptors and MLP, FP64
+ * energy and virial reductions) without relaxing: the batched counterpart
+ * of CELL_FRC (src/cmod.c:153-191) over RELX_INT's members.  Layout and
+ * limits as mb_relax_batch (nat[s] <= 64, at most 96 neighbours per atom);
+ * x Cartesian.  Outputs: H[S] enthalpies (E + pV), frc[3 * sum nat] forces,
+ * str[6S] virials U (may be NULL).  No noise zeroing.  Stated error of the
+ * FP32 evaluation against mb_efs: at most 1e-5 eV/atom in energy and
+ * 1e-4 eV/A in force. */
+int mb_efs_batch(mb_potential *pot, int S, const int *nat, const int *atmn, const double *lat, const double *x,
+                 double p_gpa, double urep, double *H, double *frc, double *str);
+
+/* ---- evolutionary search hand-off (src/emod.c) ---- */
+
+/* The batched drop-in for RELX_INT (src/emod.c:521-548): relax S offspring
+ * in one mb_relax_batch launch and write member p0 + s of generation gen to
+ * <evos_dir>/G%03d/M%03d/ as the reference leaves it for RELX_TR
+ * (src/emod.c:710-718): POSCAR.0 (the structure before relaxing),
+ * CONTCAR.0 (after; SAVE_CELL's layout, src/util.c:991-1060), OSZICAR.0
+ * (the enthalpy line Read_OSZI reads, src/util.c:1130-1147) and OUTCAR.0
+ * (CELL_OUT's final block with forces and stress, src/cmod.c:617-685).
+ * Arguments and in-place updates as mb_relax_batch; atoms of each structure
+ * grouped by species.  Species symbols are the model's. */
+int mb_evos_relax(mb_potential *pot, const char *evos_dir, int gen, int p0, int S, const int *nat, const int *atmn,
+                  double *lat, double *x, double p_gpa, double urep, int rlxt, int mitr, double fmax, double *H,
+                  int *iters, int *status);
+
+/* Write one member's four files (no GPU needed): spcz[nspc] atomic numbers
+ * of the species indices in atmn; lat0/x0 before and lat/x after relaxing
+ * (Cartesian); H enthalpy and E energy (eV); frc[3N] and str[6] (virial, eV)
+ * may be NULL; iters goes to OUTCAR's iteration line. */
+int mb_evos_write(const char *evos_dir, int gen, int member, int N, int nspc, const int *spcz, const int *atmn,
+                  const double *lat0, const double *x0, const double *lat, const double *x, double H, double E,
+                  double p_gpa, const double *frc, const double *str, int iters);
+
+/* RANK_TR's ranking (src/emod.c:304-393) of M members: order[k] = member
+ * of rank k (lowest first, ties in member order) and, if fit != NULL, the
+ * fitness fit[p] = (1 - tanh(2 (e_p - e_min) / (e_max - e_min) - 1)) / 2.
+ * e_p = H[p] as the reference ranks (total enthalpy), or H[p] / nat[p]
+ * with per_atom = 1 for populations of different sizes.  MB_ERR_STATE if
+ * e_max - e_min < 1e-12 (the reference exits there). */
+int mb_evos_rank(int M, const double *H, const int *nat, int per_atom, int *order, double *fit);
+
+/* Per-species-pair radial distribution of S structures as RANK_TR's
+ * duplicate test computes it (RDF, src/cell.c:369-417), on CUDA device
+ * `device`: every (atom, image) pair within rmax with species(j) >=
+ * species(i) adds exp(-(r - x_k)^2 / (2 sigma^2)) to the bins x_k = k rmax /
+ * nbins within 3 sigma of r, times 1 below rmin and cos(pi/2 (x_k - rmin) /
+ * (rmax - rmin)) above; same-species blocks halved; with normalise the whole
+ * vector has unit length (RDF(C, 1)).  The reference uses nbins = 3000,
+ * rmin 5.8, rmax 6.0, sigma 0.008 (src/util.c:1408-1410, src/cell.c:38).
+ * Structures as mb_relax_batch (x Cartesian, ND periodic directions);
+ * output rdf[S][nspc (nspc + 1) / 2][nbins], pairs m <= n row-major. */
+int mb_rdf(int device, int S, const int *nat, const int *atmn, const double *lat, const double *x, int ND, int nspc,
+           int nbins, double rmin, double rmax, double sigma, int normalise, double *rdf);
+
+/* Overlaps of all pairs of S vectors of length len (CxC, src/cell.c:419-430,
+ * for every pair of members at once): cxc[p*S + q] = sum_t rdf[p][t] rdf[q][t]. */
+int mb_rdf_overlap(int device, int S, int len, const double *rdf, double *cxc);
+
+/* RANK_TR's duplicate rule (src/emod.c:351-368) on M members in rank order:
+ * for p from the worst up, the first better member k with COMP_CL(p, k) =
+ * 0.8 cxc[p][k] + 0.1 exp(-(H_p - H_k)^2 / (2 0.05^2)) + 0.1 exp(-dv^2 /
+ * (2 0.01^2)) > cut, dv = (V_p - V_k) / (2 (V_p + V_k)) (src/eutl.c:394-413),
+ * marks p a duplicate: fit[p] *= 0.001 + (1 - COMP_CL)^2. */
+int mb_evos_duplicates(int M, const double *cxc, const double *H, const double *vol, double cut, double *fit);
 
 /* NVT molecular dynamics with the reference's thermostat (the RUNT == 2
  * branch of Dynamics, src/cmod.c:403-407, 440-453), entirely on the GPU:

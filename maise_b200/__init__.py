@@ -55,11 +55,21 @@ def load_library():
     lib.mb_energy.argtypes = [vp, c_i, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, _D, _D, _D]
     lib.mb_descriptors.argtypes = [vp, c_i, c_i, c_i, c_i, _I, _D, _D, _D]
     lib.mb_descriptor_vjp.argtypes = [vp, c_i, c_i, c_i, c_i, _I, _D, _D, _D, _D, _D]
+    lib.mb_neighbours.argtypes = [vp, c_i, c_i, c_i, c_i, _I, _D, _D, c_i, c_i, _I, _I, _I, _D]
     lib.mb_relax.argtypes = [vp, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _D, _L]
     lib.mb_md_nvt.argtypes = [vp, c_i, c_i, c_i, _I, _D, _D, _D, c_d, c_d, c_d, c_i, c_d, _D, _D, _D]
     lib.mb_maxwell.argtypes = [c_i, _D, c_d, ctypes.c_long, _D]
     lib.mb_relax_fmax.argtypes = [vp, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _D, _L, _I]
     lib.mb_relax_batch.argtypes = [vp, c_i, _I, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _D, _I, _I]
+    lib.mb_efs_batch.argtypes = [vp, c_i, _I, _I, _D, _D, c_d, c_d, _D, _D, _D]
+    lib.mb_evos_write.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _I, _D, _D, _D, _D, c_d, c_d, c_d, _D, _D,
+                                  c_i]
+    lib.mb_evos_relax.argtypes = [vp, ctypes.c_char_p, c_i, c_i, c_i, _I, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _D, _I,
+                                  _I]
+    lib.mb_evos_rank.argtypes = [c_i, _D, _I, c_i, _I, _D]
+    lib.mb_evos_duplicates.argtypes = [c_i, _D, _D, _D, c_d, _D]
+    lib.mb_rdf.argtypes = [c_i, c_i, _I, _I, _D, _D, c_i, c_i, c_i, c_d, c_d, c_d, c_i, _D]
+    lib.mb_rdf_overlap.argtypes = [c_i, c_i, c_i, _D, _D]
     lib.mb_batch_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), _D]
     lib.mb_atomic_mass.restype = c_d
     lib.mb_atomic_mass.argtypes = [c_i]
@@ -243,6 +253,24 @@ class Potential:
                                                _dp(g), _dp(F), _dp(U)))
         return F.reshape(N, 3), U
 
+    def neighbours(self, X, LAT, atmn, ND=3, NM=512, XT=1, path=0, cap=None):
+        """The neighbour list of the E/F/S passes (LIST's set):
+        (nn[N], nj[N,cap], shift[N,cap,3] integer images, X[N,3] wrapped).
+        path 0 as the passes choose, 1 all-pairs search, 2 cell list."""
+        atmn = _i32(atmn)
+        N = len(atmn)
+        X = _f64(X, 3 * N)
+        LAT = _f64(LAT, 9)
+        cap = cap or NM
+        nn = np.zeros(N, np.int32)
+        nj = np.zeros(N * cap, np.int32)
+        sh = np.zeros(N * cap * 3, np.int32)
+        Xw = np.zeros(3 * N)
+        self._check(self.lib.mb_neighbours(self.h, N, NM, ND, XT, atmn.ctypes.data_as(_I), _dp(LAT), _dp(X), path,
+                                           cap, nn.ctypes.data_as(_I), nj.ctypes.data_as(_I),
+                                           sh.ctypes.data_as(_I), _dp(Xw)))
+        return nn, nj.reshape(N, cap), sh.reshape(N, cap, 3), Xw.reshape(N, 3)
+
     def relax(self, X, LAT, atmn, ND=3, NM=512, p_gpa=0.0, urep=0.0, rlxt=3, mitr=100, etol=1e-6):
         """dict(H, X, LAT, n_energy, n_force, iters) -- CELL_RELX/CELL_MIN."""
         atmn = _i32(atmn)
@@ -290,6 +318,22 @@ class Potential:
         offs = np.concatenate([[0], np.cumsum(nat)])
         return dict(H=H, X=[X[offs[k]:offs[k + 1]] for k in range(S)], LAT=LAT, iters=iters, status=status,
                     evals=int(ev.value), ms=float(ms.value))
+
+    def efs_batch(self, structures, p_gpa=0.0, urep=0.0):
+        """FP32 batched E/F/S of a list of dict(X, LAT, atmn), no relaxation.
+        Returns dict(H[S], F list of [N,3], U[S,6])."""
+        nat = np.array([len(s["atmn"]) for s in structures], np.int32)
+        atmn = np.ascontiguousarray(np.concatenate([np.asarray(s["atmn"], np.int32) for s in structures]))
+        X = np.ascontiguousarray(np.concatenate([np.asarray(s["X"], float).reshape(-1, 3) for s in structures]))
+        LAT = np.ascontiguousarray(np.stack([np.asarray(s["LAT"], float).reshape(3, 3) for s in structures]))
+        S = len(structures)
+        H = np.zeros(S)
+        F = np.zeros_like(X)
+        U = np.zeros((S, 6))
+        self._check(self.lib.mb_efs_batch(self.h, S, nat.ctypes.data_as(_I), atmn.ctypes.data_as(_I), _dp(LAT),
+                                          _dp(X), p_gpa, urep, _dp(H), _dp(F), _dp(U)))
+        offs = np.concatenate([[0], np.cumsum(nat)])
+        return dict(H=H, F=[F[offs[k]:offs[k + 1]] for k in range(S)], U=U)
 
     def maxwell(self, atmn, T, seed=1):
         """Initial velocities of the reference's Maxwell() for model species atmn."""

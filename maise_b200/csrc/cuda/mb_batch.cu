@@ -70,6 +70,9 @@ struct BArgs {
     const int *order; /* queue position -> structure (largest first) */
     double *lat, *x, *H;
     int *iters, *status;
+    /* optional: forces [3 * atoms] and virial U [6 * S] at each structure's
+     * final state (FP32 evaluation, FP64 reductions); NULL to skip */
+    double *fout, *uout;
     const BParams *P;
     const float *W;
     int *queue;
@@ -890,6 +893,7 @@ __device__ double eval_finish(const BArgs &A, BShared<W> &sh, double *gout) {
                         L[1] * L[3] * L[8] - L[2] * L[4] * L[6]);
         double pv = A.p_ev * V;
         sh.scal[0] = E + pv;
+        sh.scal[4] = pv;
         for (int q = 0; q < 3; q++) U[q] -= pv;
         for (int k = 0; k < 6; k++) sh.uvir[k] = U[k];
         double mu = 0.0;
@@ -1230,6 +1234,14 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
             first = 0;
             if (maxf < A.fmax && maxu < A.fmax) status = 0;
         }
+        /* forces and virial of the final state, on request: the last
+         * evaluation was at the final DOF vector only if no step was taken */
+        if (A.fout) {
+            if (iter > 0) f = evaluate<W, C>(A, sh, sh.x, sh.g);
+            for (int k = tid; k < 3 * N; k += blockDim.x) A.fout[3 * (size_t)o + k] = (double)sh.F[k];
+            if (A.uout && tid < 6) A.uout[6 * (size_t)s + tid] = sh.uvir[tid] + (tid < 3 ? sh.scal[4] : 0.0);
+            __syncthreads();
+        }
         /* results: Cartesian positions of the final DOF vector */
         if (tid == 0) {
             if (rlxt == 3) {
@@ -1354,8 +1366,8 @@ static cudaError_t batch_launch(int units, cudaStream_t st, const BArgs &a) {
 
 extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const int *d_off, const int *d_spc,
                                const int *d_order, double *d_lat, double *d_x, double p_ev, double urep, int rlxt, int mitr, double fmax,
-                               double *d_H, int *d_iters, int *d_status, void *stream, long long *evals_out,
-                               float *ms_out) {
+                               double *d_H, int *d_iters, int *d_status, double *d_frc, double *d_str,
+                               void *stream, long long *evals_out, float *ms_out) {
     cudaStream_t st = (cudaStream_t)stream;
     BParams hp;
     float *hw = nullptr;
@@ -1420,6 +1432,7 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
         a.p_ev = p_ev; a.urep = urep; a.fmax = fmax; a.sigma = 0.1;
         a.nat = d_nat; a.off = d_off; a.spc = d_spc; a.order = d_order;
         a.lat = d_lat; a.x = d_x; a.H = d_H; a.iters = d_iters; a.status = d_status;
+        a.fout = d_frc; a.uout = d_str;
         a.P = dp; a.W = dw; a.queue = queue; a.hmat = hm; a.nbd = nbd; a.nbj = nbj; a.evals = evals;
         cudaEventRecord(e0, st);
         e = !wide        ? batch_launch<4, 1>(gunits, st, a)

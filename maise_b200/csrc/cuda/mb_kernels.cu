@@ -82,9 +82,16 @@ __device__ __forceinline__ double image_disp(const mb_cell &c, const double *xi,
     return r;
 }
 
+/* key of a list entry for the leg-table path: atom j and its integer image
+ * (5 bits per axis, two's complement) */
+__device__ __forceinline__ unsigned entry_key(int j, int i0, int i1, int i2) {
+    return ((unsigned)j << 15) | (((unsigned)i0 & 31u) << 10) | (((unsigned)i1 & 31u) << 5) | ((unsigned)i2 & 31u);
+}
+
 /* one warp per atom; candidates in the reference's order (j, then images) */
 __global__ void k_nlist_brute(int N, int NM, int cap, const double *__restrict__ X, mb_cell c, double rc2,
-                              int *__restrict__ nn, int *__restrict__ nj, double4 *__restrict__ nd, int *status) {
+                              int *__restrict__ nn, int *__restrict__ nj, double4 *__restrict__ nd, int *status,
+                              unsigned *__restrict__ nk) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= N) return;
     int i = warp;
@@ -96,15 +103,15 @@ __global__ void k_nlist_brute(int N, int NM, int cap, const double *__restrict__
     for (long long base = 0; base < total; base += 32) {
         long long cidx = base + lane;
         bool ok = false;
-        int j = 0;
+        int j = 0, i0 = 0, i1 = 0, i2 = 0;
         double d[3] = {0, 0, 0}, r2 = 0.0;
         if (cidx < total) {
             j = (int)(cidx / nimg);
             int im = (int)(cidx % nimg);
-            int i2 = im % w2 - c.Nq[2];
+            i2 = im % w2 - c.Nq[2];
             int t = im / w2;
-            int i1 = t % w1 - c.Nq[1];
-            int i0 = t / w1 - c.Nq[0];
+            i1 = t % w1 - c.Nq[1];
+            i0 = t / w1 - c.Nq[0];
             if (!(j == i && i0 == 0 && i1 == 0 && i2 == 0)) {
                 double xj[3] = {X[3 * j], X[3 * j + 1], X[3 * j + 2]};
                 r2 = image_disp(c, xi, xj, i0, i1, i2, d);
@@ -116,6 +123,7 @@ __global__ void k_nlist_brute(int N, int NM, int cap, const double *__restrict__
         if (ok && pos < cap) {
             nj[(size_t)i * cap + pos] = j;
             nd[(size_t)i * cap + pos] = make_double4(d[0], d[1], d[2], sqrt(r2));
+            if (nk) nk[(size_t)i * cap + pos] = entry_key(j, i0, i1, i2);
         }
         count += __popc(m);
     }
@@ -201,7 +209,7 @@ __global__ void k_cell_sort(int ncell, const int *start, int *atoms) {
 __global__ void k_nlist_cell(int N, int NM, int cap, const double *__restrict__ X, mb_cell c, double rc2,
                              const int *__restrict__ cell_of, const int *__restrict__ start,
                              const int *__restrict__ atoms, int *__restrict__ nn, int *__restrict__ nj,
-                             double4 *__restrict__ nd, int *status) {
+                             double4 *__restrict__ nd, int *status, unsigned *__restrict__ nk) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= N) return;
     int i = warp;
@@ -246,6 +254,7 @@ __global__ void k_nlist_cell(int N, int NM, int cap, const double *__restrict__ 
                     if (ok && pos < cap) {
                         nj[(size_t)i * cap + pos] = j;
                         nd[(size_t)i * cap + pos] = make_double4(d[0], d[1], d[2], sqrt(r2));
+                        if (nk) nk[(size_t)i * cap + pos] = entry_key(j, img[0], img[1], img[2]);
                     }
                     count += __popc(m);
                 }
@@ -459,8 +468,8 @@ __device__ __forceinline__ void group_sync() {
 
 /* Reduction of a 64-cell accumulator grid over the atom's group into
  * s.red[0..63] (warp 0 adds the warps' partial sums in a fixed order). */
-template <int WPA>
-__device__ __forceinline__ void group_reduce64(double *v, EfsSmem &s, int gwarp, int lane) {
+template <int WPA, class Smem>
+__device__ __forceinline__ void group_reduce64(double *v, Smem &s, int gwarp, int lane) {
     warp_reduce64(v, lane);
     if (WPA == 1) {
         s.red[2 * lane] = v[0];
@@ -486,8 +495,8 @@ __device__ __forceinline__ void group_reduce64(double *v, EfsSmem &s, int gwarp,
 
 /* As group_reduce64 for values already summed over the warp (lane l holds
  * cells 2l and 2l+1, the layout of a tensor-core accumulator fragment). */
-template <int WPA>
-__device__ __forceinline__ void group_store64(double v0, double v1, EfsSmem &s, int gwarp, int lane) {
+template <int WPA, class Smem>
+__device__ __forceinline__ void group_store64(double v0, double v1, Smem &s, int gwarp, int lane) {
     if (WPA == 1) {
         s.red[2 * lane] = v0;
         s.red[2 * lane + 1] = v1;
@@ -1145,6 +1154,691 @@ __global__ void __launch_bounds__(WPA * 32 * APB, APB >= 4 ? 2 : 1) k_efs(EfsArg
 }
 
 /* ------------------------------------------------------------------ */
+/* leg-table path of the descriptor pass                                */
+/* ------------------------------------------------------------------ */
+
+/* A triplet (i; j, k) of PRS_BP has three legs, i-j, i-k and j-k, and each
+ * leg's factors -- exp(-eta_e r^2) for the G4 exponents and the cutoff fc(r)
+ * (src/nprs.c:540-547) -- depend only on that pair.  The j-k leg is an entry
+ * of j's own neighbour list, and each such entry serves every atom that has
+ * both j and k as neighbours (about 29 triplets in a dense alloy).  k_legs
+ * evaluates the factors once per list entry; k_efs_leg reads the j-k leg of
+ * each triplet from j's row instead of evaluating it, and finds that row by
+ * walking j's list and looking each entry up in a hash of i's own entries
+ * keyed by (atom, image).  The walk enumerates exactly the triplets with
+ * both r_ik < Rc (k is found in i's list) and r_jk < Rc (k is in j's list).
+ *
+ * The path applies to bases whose forward and derivative functions share one
+ * cutoff and whose pair-mixed G4 exponents equal the species-0 ones (every
+ * reference model; src/nprs.c:222-252 mixes identical blocks), so a leg's
+ * factors serve the energy and the derivative terms alike. */
+
+#define LEG_PER_LANE (MB_LEG_MAX_CAP / 32)
+#define LEG_HASH 256 /* hash slots per atom: at least twice the neighbour capacity */
+
+__device__ __forceinline__ int sx5(unsigned v) { return (int)((v & 31u) ^ 16u) - 16; }
+
+/* One warp per atom: sort the atom's entries stably by the neighbour's
+ * species (in place: nj, nk, nd), record where each species starts
+ * (nso[4i+s]; nso[4i+3] = count), and write each entry's leg row with the
+ * forward parameters of the pair (i, j): exp(-eta_e r^2) for e < ne (0
+ * above), fc(r) and fc'(r)/r at the G4 cutoff. */
+__global__ void k_legs(int N, int cap, const int *__restrict__ nn, int *__restrict__ nj, unsigned *__restrict__ nk,
+                       double4 *__restrict__ nd, const int *__restrict__ spc, const mb_params *__restrict__ Pg,
+                       double *__restrict__ leg, int *__restrict__ nso) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= N) return;
+    const int i = warp, n = nn[i], s0 = spc[i], ne = Pg->ne;
+    const size_t row = (size_t)i * cap;
+    int jv[LEG_PER_LANE], spv[LEG_PER_LANE];
+    unsigned kv[LEG_PER_LANE];
+    double4 dv[LEG_PER_LANE];
+    int cnt[MB_MAXSPC] = {0, 0, 0};
+#pragma unroll
+    for (int q = 0; q < LEG_PER_LANE; q++) {
+        const int t = q * 32 + lane;
+        spv[q] = -1;
+        jv[q] = 0;
+        kv[q] = 0u;
+        dv[q] = make_double4(0.0, 0.0, 0.0, 1.0);
+        if (t < n) {
+            jv[q] = nj[row + t];
+            kv[q] = nk[row + t];
+            dv[q] = nd[row + t];
+            spv[q] = spc[jv[q]];
+        }
+#pragma unroll
+        for (int v = 0; v < MB_MAXSPC; v++) cnt[v] += __popc(__ballot_sync(FULL, spv[q] == v));
+    }
+    int off[MB_MAXSPC + 1];
+    off[0] = 0;
+#pragma unroll
+    for (int v = 0; v < MB_MAXSPC; v++) off[v + 1] = off[v] + cnt[v];
+    if (lane < 4) nso[4 * i + lane] = off[lane];
+    __syncwarp();
+    const unsigned below = (1u << lane) - 1u;
+    int run[MB_MAXSPC] = {0, 0, 0};
+#pragma unroll
+    for (int q = 0; q < LEG_PER_LANE; q++) {
+        int dst = 0;
+#pragma unroll
+        for (int v = 0; v < MB_MAXSPC; v++) {
+            const unsigned m = __ballot_sync(FULL, spv[q] == v);
+            if (spv[q] == v) dst = off[v] + run[v] + __popc(m & below);
+            run[v] += __popc(m);
+        }
+        if (spv[q] >= 0) {
+            nj[row + dst] = jv[q];
+            nk[row + dst] = kv[q];
+            nd[row + dst] = dv[q];
+            const int p = s0 * s0 + spv[q] * spv[q];
+            const double r = dv[q].w;
+            double f, df;
+            fcut_d(Pg->f_rc4[p], r, f, df);
+            double e[MB_LEG_STRIDE];
+#pragma unroll
+            for (int k = 0; k < 8; k++) e[k] = k < ne ? exp(-Pg->f_eta4[p][k] * r * r) : 0.0;
+            e[8] = f;
+            e[9] = df / r;
+            double2 *o = reinterpret_cast<double2 *>(leg + (row + dst) * MB_LEG_STRIDE);
+#pragma unroll
+            for (int k = 0; k < MB_LEG_STRIDE / 2; k++) o[k] = make_double2(e[2 * k], e[2 * k + 1]);
+        }
+    }
+}
+
+struct LegArgs {
+    int N, cap, mode;
+    double urep;
+    const int *nn, *nj, *nso;
+    const unsigned *nk;
+    const double4 *nd;
+    const double *leg;
+    const int *spc;
+    const mb_params *params;
+    const double *weights;
+    double *EA, *EU, *G, *F, *vir;
+    unsigned long long *counters;
+    size_t smem_group;
+    int tl_cap;
+};
+
+/* shared-memory carve-up of one atom group of k_efs_leg */
+struct LegSmem {
+    double *stage;                          /* tensor-core staging (forward) | */
+    double *Fnb, *grid, *red, *h;           /* reductions, MLP, reverse pass   */
+    double4 *d;
+    double *ir, *L, *G;
+    double *tmp;                            /* G2 terms | */
+    unsigned *tl;                           /* triplet list */
+    uint2 *hash;
+    int *j, *sp, *jo, *blk, *seg;
+    unsigned *key;
+};
+
+__host__ __device__ inline size_t leg_smem_bytes(int cap, int D, int ng2, int warps, int tl) {
+    size_t b = efs_union_bytes(cap, 64, warps, 1);
+    b += sizeof(double4) * cap;
+    b += sizeof(double) * cap;                        /* ir */
+    b += sizeof(double) * cap * MB_LEG_STRIDE;        /* L */
+    b += align16(sizeof(double) * D);                 /* G */
+    const size_t tmp_b = sizeof(double) * cap * (ng2 > 1 ? ng2 : 1), tl_b = align16(sizeof(unsigned) * tl);
+    b += align16(tmp_b > tl_b ? tmp_b : tl_b);        /* tmp | tl */
+    b += sizeof(uint2) * LEG_HASH;
+    b += align16(sizeof(int) * cap) * 3;              /* j, sp, key */
+    b += sizeof(int) * 4 * cap;                       /* jo */
+    b += align16(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
+    b += sizeof(int) * 8;
+    return align16(b);
+}
+
+__device__ inline LegSmem leg_carve(char *base, int cap, int D, int ng2, int warps, int tl) {
+    LegSmem s;
+    char *p = base;
+    s.stage = (double *)p;
+    s.Fnb = (double *)p;
+    s.grid = s.Fnb + cap * 3;
+    s.red = s.grid + 64;
+    s.h = s.red + warps * 64;
+    p += efs_union_bytes(cap, 64, warps, 1);
+    s.d = (double4 *)p; p += sizeof(double4) * cap;
+    s.ir = (double *)p; p += sizeof(double) * cap;
+    s.L = (double *)p; p += sizeof(double) * cap * MB_LEG_STRIDE;
+    s.G = (double *)p; p += align16(sizeof(double) * D);
+    {
+        const size_t tmp_b = sizeof(double) * cap * (ng2 > 1 ? ng2 : 1), tl_b = align16(sizeof(unsigned) * tl);
+        s.tmp = (double *)p;
+        s.tl = (unsigned *)p;
+        p += align16(tmp_b > tl_b ? tmp_b : tl_b);
+    }
+    s.hash = (uint2 *)p; p += sizeof(uint2) * LEG_HASH;
+    s.j = (int *)p; p += align16(sizeof(int) * cap);
+    s.sp = (int *)p; p += align16(sizeof(int) * cap);
+    s.key = (unsigned *)p; p += align16(sizeof(int) * cap);
+    s.jo = (int *)p; p += sizeof(int) * 4 * cap;
+    s.blk = (int *)p; p += align16(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
+    s.seg = (int *)p;
+    return s;
+}
+
+__device__ __forceinline__ unsigned hash_slot(unsigned key) { return (key * 0x9E3779B1u) >> 24; }
+
+/* slot of the staged entry with this key, or -1 (linear probing, bounded) */
+__device__ __forceinline__ int hash_find(const LegSmem &s, unsigned key) {
+    unsigned h = hash_slot(key);
+    for (int probe = 0; probe < LEG_HASH; probe++) {
+        const uint2 e = s.hash[h];
+        if (e.x == key) return (int)e.y;
+        if (e.x == 0xffffffffu) return -1;
+        h = (h + 1u) & (LEG_HASH - 1u);
+    }
+    return -1;
+}
+
+/* Each lane's position (a, c) in the candidate legs of one species block:
+ * for the staged neighbours a in [.., a_hi) of the block's first species,
+ * the entries c of a's own list whose atom has absolute species sb. */
+struct LegCur {
+    int a, c;
+};
+
+__device__ __forceinline__ void leg_norm(const LegSmem &s, LegCur &u, int a_hi, int sb) {
+    while (u.a < a_hi) {
+        const int len = s.jo[4 * u.a + sb + 1] - s.jo[4 * u.a + sb];
+        if (u.c < len) break;
+        u.c -= len;
+        u.a++;
+    }
+}
+
+/* Append the block's accepted triplets (a, b, c) -- b > a, the entry c of
+ * a's list being atom k at the image that puts it at i's slot b -- to this
+ * warp's list region as a | b << 8 | c << 16, 32 candidates per round, the
+ * warps of an atom taking every WPA-th round.  Stops when the region
+ * cannot take another round; returns 1 once the block is exhausted. */
+template <int WPA>
+__device__ __forceinline__ int leg_fill(const LegSmem &s, const unsigned *__restrict__ nk, int cap, int a_hi, int sb,
+                                        LegCur &u, int &pos, int hi, int lane) {
+    for (;;) {
+        const bool live = u.a < a_hi;
+        if (!__any_sync(FULL, live)) return 1;
+        if (pos + 32 > hi) return 0;
+        bool ok = false;
+        unsigned ent = 0u;
+        if (live) {
+            const int a = u.a, c = s.jo[4 * a + sb] + u.c;
+            const unsigned kc = __ldg(nk + (size_t)s.j[a] * cap + c), ka = s.key[a];
+            const int x0 = sx5(ka >> 10) + sx5(kc >> 10), x1 = sx5(ka >> 5) + sx5(kc >> 5), x2 = sx5(ka) + sx5(kc);
+            if (x0 >= -16 && x0 <= 15 && x1 >= -16 && x1 <= 15 && x2 >= -16 && x2 <= 15) {
+                const unsigned key =
+                    (kc & ~0x7fffu) | (((unsigned)x0 & 31u) << 10) | (((unsigned)x1 & 31u) << 5) | ((unsigned)x2 & 31u);
+                const int b = hash_find(s, key);
+                ok = b > a;
+                ent = (unsigned)a | ((unsigned)b << 8) | ((unsigned)c << 16);
+            }
+        }
+        const unsigned m = __ballot_sync(FULL, ok);
+        if (ok) s.tl[pos + __popc(m & ((1u << lane) - 1u))] = ent;
+        pos += __popc(m);
+        u.c += 32 * WPA;
+        leg_norm(s, u, a_hi, sb);
+    }
+}
+
+/* body(ent, valid) over list entries [from, to) with the warp converged */
+template <class Body>
+__device__ __forceinline__ void leg_run_all(const LegSmem &s, int from, int to, int lane, Body body) {
+    for (int base = from; base < to; base += 32) {
+        const int t = base + lane;
+        const bool valid = t < to;
+        body(valid ? s.tl[t] : 0u, valid);
+    }
+}
+
+/* body(ent) -> the entry's force on neighbour a, over entries [from, to):
+ * each lane takes a contiguous run of K entries (K odd, so that the lanes'
+ * list reads fall in distinct banks); consecutive entries mostly share a,
+ * so the a-side forces are summed in registers and added to Fnb once per
+ * change of a. */
+template <class Body>
+__device__ __forceinline__ void leg_run_runs(const LegSmem &s, int from, int to, int lane, Body body) {
+    int K = (to - from + 31) >> 5;
+    if (K > 0) K |= 1;
+    const int t0 = from + lane * K;
+    int ca = -1;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int step = 0; step < K; step++) {
+        const int t = t0 + step;
+        if (t >= to) break;
+        const unsigned ent = s.tl[t];
+        const int a = (int)(ent & 0xffu);
+        if (a != ca) {
+            if (ca >= 0) {
+                atomicAdd(&s.Fnb[3 * ca], -sx);
+                atomicAdd(&s.Fnb[3 * ca + 1], -sy);
+                atomicAdd(&s.Fnb[3 * ca + 2], -sz);
+            }
+            ca = a;
+            sx = sy = sz = 0.0;
+        }
+        const double3 g = body(ent);
+        sx += g.x;
+        sy += g.y;
+        sz += g.z;
+    }
+    if (ca >= 0) {
+        atomicAdd(&s.Fnb[3 * ca], -sx);
+        atomicAdd(&s.Fnb[3 * ca + 1], -sy);
+        atomicAdd(&s.Fnb[3 * ca + 2], -sz);
+    }
+}
+
+/* Enumerate block (alpha, beta) for this warp and run `body` over its
+ * triplets: from the stored entries [blk[0], blk[1]) when `reuse`, else
+ * filling the region (in rounds when it overflows).  Records the range and
+ * returns 0 if the region overflowed (the range is then not reusable). */
+template <int WPA, int RUN, class Body>
+__device__ __forceinline__ int leg_block(const LegSmem &s, const unsigned *__restrict__ nk, int cap, int a_lo, int a_hi,
+                                         int sb, int *blk, int reuse, int &pos, int lo, int hi, int warp, int lane,
+                                         Body body) {
+    if (reuse) {
+        if constexpr (RUN == RUN_CONVERGED)
+            leg_run_all(s, blk[0], blk[1], lane, body);
+        else
+            leg_run_runs(s, blk[0], blk[1], lane, body);
+        return 1;
+    }
+    LegCur u{a_lo, warp * 32 + lane};
+    leg_norm(s, u, a_hi, sb);
+    int start = pos, whole = 1;
+    for (;;) {
+        const int from = pos;
+        const int done = leg_fill<WPA>(s, nk, cap, a_hi, sb, u, pos, hi, lane);
+        __syncwarp();
+        if constexpr (RUN == RUN_CONVERGED)
+            leg_run_all(s, from, pos, lane, body);
+        else
+            leg_run_runs(s, from, pos, lane, body);
+        __syncwarp();
+        if (done) break;
+        whole = 0; /* region full: restart it for the next round */
+        start = pos = lo;
+    }
+    blk[0] = start;
+    blk[1] = pos;
+    return whole;
+}
+
+/* The fused descriptor / MLP / force kernel on leg tables: the stages of
+ * k_efs with every triplet's leg factors read from the rows k_legs wrote
+ * (i-j and i-k from i's own rows, staged; j-k from j's row in global
+ * memory, L2-resident).  Reference bases: at most 8 G4 exponents, zeta in
+ * {1, 2, 4, 16} or other integers, 2 lambdas. */
+template <int WPA, int APB>
+__global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
+    constexpr int NZ = 4, NLAM = 2, NZL = 8, NE = 8;
+    extern __shared__ __align__(16) char smem_raw[];
+    __shared__ mb_params Ps;
+    {
+        const int *src = reinterpret_cast<const int *>(A.params);
+        int *dst = reinterpret_cast<int *>(&Ps);
+        for (int k = threadIdx.x; k < (int)(sizeof(mb_params) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+        __syncthreads();
+    }
+    const mb_params &P = Ps;
+    const int NT = WPA * 32, group = threadIdx.x / NT;
+    const int tid = threadIdx.x % NT, lane = threadIdx.x & 31, warp = tid >> 5;
+    const int i = blockIdx.x * APB + group;
+    if (i >= A.N) return; /* whole atom groups only: no barrier spans two groups */
+    const int D = P.D, ns = P.nspc, ng2 = P.ng2, ne = P.ne, cap = A.cap;
+    LegSmem s = leg_carve(smem_raw + (size_t)group * A.smem_group, cap, D, ng2, WPA, A.tl_cap);
+    const int tlw = A.tl_cap / WPA, tl_lo = warp * tlw, tl_hi = tl_lo + tlw;
+    int tl_pos = tl_lo, tl_whole = 1;
+    const int n = A.nn[i];
+    const int s0 = A.spc[i];
+    const double *net = A.weights + P.w_off[s0];
+    const size_t row = (size_t)i * cap;
+
+    /* ---- stage i's entries in relative-species order (k_legs sorted them by
+     * absolute species: relative species v is absolute (s0 + v) % ns) ---- */
+    if (tid < 4) {
+        const int v = tid, sa = (s0 + v) % ns;
+        int c = 0, o = 0;
+        if (v < ns) c = A.nso[4 * i + sa + 1] - A.nso[4 * i + sa];
+        for (int w = 0; w < v; w++) {
+            const int sw = (s0 + w) % ns;
+            o += A.nso[4 * i + sw + 1] - A.nso[4 * i + sw];
+        }
+        s.seg[v] = c;
+        s.seg[4 + v] = v < ns ? o : n;
+    }
+    for (int t = tid; t < D; t += NT) s.G[t] = 0.0;
+    for (int t = tid; t < LEG_HASH; t += NT) s.hash[t] = make_uint2(0xffffffffu, 0u);
+    group_sync<WPA>();
+    for (int u = tid; u < n; u += NT) {
+        int v = 0;
+        while (v + 1 < ns && u >= s.seg[4 + v + 1]) v++;
+        const int sa = (s0 + v) % ns;
+        const int t = A.nso[4 * i + sa] + (u - s.seg[4 + v]);
+        const int j = A.nj[row + t];
+        const double4 dv = A.nd[row + t];
+        s.j[u] = j;
+        s.sp[u] = sa;
+        s.key[u] = A.nk[row + t];
+        s.d[u] = dv;
+        s.ir[u] = 1.0 / dv.w;
+        const double2 *src = reinterpret_cast<const double2 *>(A.leg + (row + t) * MB_LEG_STRIDE);
+        double2 *dst = reinterpret_cast<double2 *>(s.L + (size_t)u * MB_LEG_STRIDE);
+#pragma unroll
+        for (int k = 0; k < MB_LEG_STRIDE / 2; k++) dst[k] = __ldg(src + k);
+        const int4 jo = *reinterpret_cast<const int4 *>(A.nso + 4 * j);
+        s.jo[4 * u] = jo.x;
+        s.jo[4 * u + 1] = jo.y;
+        s.jo[4 * u + 2] = jo.z;
+        s.jo[4 * u + 3] = jo.w;
+    }
+    group_sync<WPA>();
+    for (int u = tid; u < n; u += NT) {
+        const unsigned key = s.key[u];
+        unsigned h = hash_slot(key);
+        for (int probe = 0; probe < LEG_HASH; probe++) {
+            if (atomicCAS(&s.hash[h].x, 0xffffffffu, key) == 0xffffffffu) {
+                s.hash[h].y = (unsigned)u;
+                break;
+            }
+            h = (h + 1u) & (LEG_HASH - 1u);
+        }
+    }
+    group_sync<WPA>();
+    if (tid == 0 && A.counters) atomicAdd(&A.counters[0], (unsigned long long)n);
+
+    if (A.mode != MB_MODE_VJP) {
+        /* ---- forward pair terms: G2 (src/nprs.c:518-526) and repulsion ---- */
+        for (int t = tid; t < n; t += NT) {
+            const double r = s.d[t].w;
+            const int p = s0 * s0 + s.sp[t] * s.sp[t];
+            const double fa = s.L[t * MB_LEG_STRIDE + 8]; /* one cutoff for all functions */
+            for (int f = 0; f < ng2; f++) {
+                const double x = r - P.f_rs[p][f];
+                s.tmp[t * ng2 + f] = fa * exp(-P.f_eta2[p][f] * (x * x));
+            }
+        }
+        group_sync<WPA>();
+        for (int w = tid; w < ns * ng2; w += NT) {
+            const int v = w / ng2, f = w % ng2;
+            double acc = 0.0;
+            for (int t = s.seg[4 + v]; t < s.seg[4 + v] + s.seg[v]; t++) acc += s.tmp[t * ng2 + f];
+            s.G[P.ind2[v] + f] = acc;
+        }
+        if (A.urep > 0.0 && tid == 0) {
+            double eu = 0.0;
+            for (int t = 0; t < n; t++) {
+                const double r = s.d[t].w, R = P.rm[s0] + P.rm[s.sp[t]];
+                if (r < R) eu += A.urep * fcut(R, r) * R / r;
+            }
+            A.EU[i] = eu;
+        }
+        group_sync<WPA>(); /* the G2 terms in tmp are read; the triplet list reuses their space */
+
+        /* ---- forward triplet terms, block by block, on the FP64 tensor cores ---- */
+        int blkid = 0;
+        unsigned long long nacc = 0;
+        for (int al = 0; al < ns; al++)
+            for (int be = al; be < ns; be++, blkid++) {
+                const int sb = (s0 + be) % ns;
+                double c0 = 0.0, c1 = 0.0;
+                double *stw = s.stage + warp * 32 * EFS_STG;
+                auto body = [&](unsigned ent, bool valid) {
+                    double ex[8], lz[NZL];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) ex[q] = 0.0;
+#pragma unroll
+                    for (int q = 0; q < NZL; q++) lz[q] = 0.0;
+                    if (valid) {
+                        nacc++;
+                        const int a = (int)(ent & 0xffu), b = (int)((ent >> 8) & 0xffu), cj = (int)(ent >> 16);
+                        const double4 d1 = s.d[a], d2 = s.d[b];
+                        const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (s.ir[a] * s.ir[b]);
+                        const double2 *la = reinterpret_cast<const double2 *>(s.L + a * MB_LEG_STRIDE);
+                        const double2 *lb = reinterpret_cast<const double2 *>(s.L + b * MB_LEG_STRIDE);
+                        const double2 *lg =
+                            reinterpret_cast<const double2 *>(A.leg + ((size_t)s.j[a] * cap + cj) * MB_LEG_STRIDE);
+                        const double A3 = 2.0 * la[4].x * lb[4].x * __ldg(lg + 4).x;
+                        angular<NZ, NLAM>(P, c, lz, nullptr);
+#pragma unroll
+                        for (int hh = 0; hh < NE / 2; hh++) {
+                            const double2 x = la[hh], y = lb[hh], z = __ldg(lg + hh);
+                            ex[2 * hh] = A3 * (x.x * y.x) * z.x;
+                            ex[2 * hh + 1] = A3 * (x.y * y.y) * z.y;
+                        }
+                    }
+                    double *rw = stw + lane * EFS_STG;
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        rw[q] = ex[q];
+                        rw[8 + q] = lz[q];
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int st = 0; st < 8; st++) {
+                        const double *r = stw + (4 * st + (lane & 3)) * EFS_STG;
+                        dmma884(c0, c1, r[lane >> 2], r[8 + (lane >> 2)]);
+                    }
+                    __syncwarp();
+                };
+                int *blk = s.blk + (blkid * WPA + warp) * 2;
+                const int a_lo = s.seg[4 + al], a_hi = a_lo + s.seg[al];
+                tl_whole &= leg_block<WPA, RUN_CONVERGED>(s, A.nk, cap, a_lo, a_hi, sb, blk, 0, tl_pos, tl_lo,
+                                                          tl_hi, warp, lane, body);
+                group_sync<WPA>();
+                group_store64<WPA>(c0, c1, s, warp, lane);
+                if (tid == 0) {
+                    const int base = P.ind4[al * al + be * be];
+                    for (int f = 0; f < P.ng4; f++)
+                        s.G[base + f] += s.red[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam];
+                }
+                group_sync<WPA>();
+            }
+        if (A.counters) {
+            for (int o = 16; o > 0; o >>= 1) nacc += __shfl_xor_sync(FULL, nacc, o);
+            if (lane == 0) atomicAdd(&A.counters[1], nacc);
+        }
+        if (A.mode == MB_MODE_DESCRIPTORS) {
+            for (int t = tid; t < D; t += NT) A.G[(size_t)i * D + t] = s.G[t];
+            return;
+        }
+    }
+
+    /* ---- MLP: forward (src/nmlp.c:367-431) and dE/dG ---- */
+    const int h1 = P.h1, h2 = P.h2;
+    const double *off = net, *W0 = off + D, *b0 = W0 + h1 * D, *W1 = b0 + h1, *b1 = W1 + h2 * h1, *W2 = b1 + h2,
+                 *b2 = W2 + h2;
+    double *H1 = s.h, *H2 = s.h + MB_MAXH, *Dl1 = s.h + 2 * MB_MAXH, *Dl2 = s.h + 3 * MB_MAXH;
+    if (A.mode != MB_MODE_VJP) {
+        for (int m = warp; m < h1; m += WPA) {
+            double acc = 0.0;
+            for (int l = lane; l < D; l += 32) acc += (s.G[l] - off[l]) * W0[m * D + l];
+            acc = warp_sum(acc);
+            if (lane == 0) H1[m] = tanh(b0[m] + acc);
+        }
+        group_sync<WPA>();
+        if (warp == 0) {
+            double v = 0.0;
+            if (lane < h2) {
+                v = b1[lane];
+                for (int k = 0; k < h1; k++) v += H1[k] * W1[lane * h1 + k];
+                v = tanh(v);
+                H2[lane] = v;
+            }
+            double e = lane < h2 ? v * W2[lane] : 0.0;
+            e = warp_sum(e);
+            if (lane == 0) A.EA[i] = b2[0] + e;
+            __syncwarp();
+            if (lane < h2) Dl2[lane] = W2[lane] * (1.0 - v * v);
+            __syncwarp();
+            if (lane < h1) {
+                double g = 0.0;
+                for (int m = 0; m < h2; m++) g += Dl2[m] * W1[m * h1 + lane];
+                Dl1[lane] = g * (1.0 - H1[lane] * H1[lane]);
+            }
+        }
+        group_sync<WPA>();
+        if (A.mode == MB_MODE_ENERGY) return;
+        for (int l = tid; l < D; l += NT) {
+            double g = 0.0;
+            for (int k = 0; k < h1; k++) g += Dl1[k] * W0[k * D + l];
+            s.G[l] = g;
+        }
+    } else {
+        for (int l = tid; l < D; l += NT) s.G[l] = A.G[(size_t)i * D + l];
+    }
+    group_sync<WPA>();
+
+    /* ---- reverse pair terms with the species-0 parameters ---- */
+    double fi[3] = {0.0, 0.0, 0.0}, vr[6] = {0, 0, 0, 0, 0, 0};
+    for (int t = tid; t < n; t += NT) {
+        const double4 d = s.d[t];
+        const double r = d.w, ir = s.ir[t];
+        double f2, df2;
+        fcut_d(P.d_rc2, r, f2, df2);
+        const int ds1 = (s.sp[t] - s0 + ns) % ns;
+        const double *g = s.G + P.ind2[ds1];
+        double cpair = 0.0;
+        for (int f = 0; f < ng2; f++) {
+            const double x = r - P.d_rs[f], eta = P.d_eta2[f];
+            cpair += g[f] * exp(-eta * x * x) * (-2.0 * eta * x * f2 + df2);
+        }
+        const double cr = cpair * ir;
+        const double v0 = cr * d.x, v1 = cr * d.y, v2 = cr * d.z;
+        fi[0] += v0; fi[1] += v1; fi[2] += v2;
+        s.Fnb[3 * t] = -v0; s.Fnb[3 * t + 1] = -v1; s.Fnb[3 * t + 2] = -v2;
+        if (A.urep > 0.0) {
+            const double R = P.rm[s0] + P.rm[s.sp[t]];
+            if (r < R) {
+                /* CELL_UREP on the ordered pair (i, j): force on i only (src/cmod.c:100-112) */
+                double fu, dfu;
+                fcut_d(R, r, fu, dfu);
+                const double tu = -2.0 * A.urep * R / (r * r) * (-fu / r + dfu);
+                fi[0] -= tu * d.x; fi[1] -= tu * d.y; fi[2] -= tu * d.z;
+                vr[0] += 0.5 * tu * d.x * d.x; vr[1] += 0.5 * tu * d.y * d.y; vr[2] += 0.5 * tu * d.z * d.z;
+                vr[3] += 0.5 * tu * d.x * d.y; vr[4] += 0.5 * tu * d.y * d.z; vr[5] += 0.5 * tu * d.z * d.x;
+            }
+        }
+    }
+    group_sync<WPA>();
+
+    /* ---- reverse triplet terms (the forward list reused) ---- */
+    {
+        const int reuse = (A.mode != MB_MODE_VJP) && tl_whole;
+        int blkid = 0;
+        tl_pos = tl_lo;
+        double eta[NE];
+#pragma unroll
+        for (int e = 0; e < NE; e++) eta[e] = e < ne ? P.d_eta4[e] : 0.0;
+        for (int al = 0; al < ns; al++)
+            for (int be = al; be < ns; be++, blkid++) {
+                const int sb = (s0 + be) % ns;
+                const int base = P.ind4[al * al + be * be];
+                for (int t = tid; t < 64; t += NT) s.grid[t] = 0.0;
+                group_sync<WPA>();
+                if (tid == 0)
+                    for (int f = 0; f < P.ng4; f++)
+                        s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam] += s.G[base + f];
+                group_sync<WPA>();
+                auto body = [&](unsigned ent) -> double3 {
+                    const int a = (int)(ent & 0xffu), b = (int)((ent >> 8) & 0xffu), cj = (int)(ent >> 16);
+                    const double4 d1 = s.d[a], d2 = s.d[b];
+                    const double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
+                    const double ir1 = s.ir[a], ir2 = s.ir[b];
+                    const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
+                    const double2 *la = reinterpret_cast<const double2 *>(s.L + a * MB_LEG_STRIDE);
+                    const double2 *lb = reinterpret_cast<const double2 *>(s.L + b * MB_LEG_STRIDE);
+                    const double2 *lg =
+                        reinterpret_cast<const double2 *>(A.leg + ((size_t)s.j[a] * cap + cj) * MB_LEG_STRIDE);
+                    const double2 fa = la[4], fb = lb[4], fg = __ldg(lg + 4);
+                    double lz[NZL], lzp[NZL];
+#pragma unroll
+                    for (int k = 0; k < NZL; k++) { lz[k] = 0.0; lzp[k] = 0.0; }
+                    angular<NZ, NLAM>(P, c, lz, lzp);
+                    double Q = 0.0, Qe = 0.0, Qc = 0.0;
+#pragma unroll
+                    for (int hh = 0; hh < NE / 2; hh++) {
+                        const double2 x = la[hh], y = lb[hh], z = __ldg(lg + hh);
+#pragma unroll
+                        for (int q = 0; q < 2; q++) {
+                            const int e = 2 * hh + q;
+                            const double E = q ? (x.y * y.y) * z.y : (x.x * y.x) * z.x;
+                            double u = 0.0, v = 0.0;
+#pragma unroll
+                            for (int zl = 0; zl < NZL; zl += 2) {
+                                const double2 cg = *reinterpret_cast<const double2 *>(s.grid + e * NZL + zl);
+                                u += cg.x * lz[zl] + cg.y * lz[zl + 1];
+                                v += cg.x * lzp[zl] + cg.y * lzp[zl + 1];
+                            }
+                            Q += E * u;
+                            Qe += eta[e] * E * u;
+                            Qc += E * v;
+                        }
+                    }
+                    /* legs: f = fc(r), h = fc'(r)/r (i-j: a, i-k: b, j-k: g) */
+                    const double Af = 2.0 * fa.x * fb.x * fg.x;
+                    const double T1 = 2.0 * fa.y * fb.x * fg.x * Q - 2.0 * Af * Qe; /* dT/dr1 / r1 */
+                    const double T2 = 2.0 * fa.x * fb.y * fg.x * Q - 2.0 * Af * Qe;
+                    const double T3 = 2.0 * fa.x * fb.x * fg.y * Q - 2.0 * Af * Qe;
+                    const double Tc = Af * Qc;
+                    const double a11 = T1 - Tc * c * ir1 * ir1, a22 = T2 - Tc * c * ir2 * ir2;
+                    const double a12 = Tc * ir1 * ir2, a3 = T3;
+                    const double g1x = a11 * d1.x + a12 * d2.x - a3 * wx;
+                    const double g1y = a11 * d1.y + a12 * d2.y - a3 * wy;
+                    const double g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
+                    const double g2x = a22 * d2.x + a12 * d1.x + a3 * wx;
+                    const double g2y = a22 * d2.y + a12 * d1.y + a3 * wy;
+                    const double g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                    fi[0] += g1x + g2x; fi[1] += g1y + g2y; fi[2] += g1z + g2z;
+                    atomicAdd(&s.Fnb[3 * b], -g2x);
+                    atomicAdd(&s.Fnb[3 * b + 1], -g2y);
+                    atomicAdd(&s.Fnb[3 * b + 2], -g2z);
+                    return make_double3(g1x, g1y, g1z);
+                };
+                int *blk = s.blk + (blkid * WPA + warp) * 2;
+                const int a_lo = s.seg[4 + al], a_hi = a_lo + s.seg[al];
+                leg_block<WPA, RUN_RUNS>(s, A.nk, cap, a_lo, a_hi, sb, blk, reuse, tl_pos, tl_lo, tl_hi, warp, lane,
+                                         body);
+                group_sync<WPA>();
+            }
+    }
+
+    /* virial of atom i's energy: every neighbour force times its displacement */
+    for (int t = tid; t < n; t += NT) {
+        const double4 d = s.d[t];
+        const double fx = s.Fnb[3 * t], fy = s.Fnb[3 * t + 1], fz = s.Fnb[3 * t + 2];
+        vr[0] += fx * d.x; vr[1] += fy * d.y; vr[2] += fz * d.z;
+        vr[3] += fx * d.y; vr[4] += fy * d.z; vr[5] += fz * d.x;
+    }
+    {
+        double v[64];
+#pragma unroll
+        for (int k = 0; k < 64; k++) v[k] = 0.0;
+        v[0] = fi[0]; v[1] = fi[1]; v[2] = fi[2];
+#pragma unroll
+        for (int k = 0; k < 6; k++) v[3 + k] = vr[k];
+        group_reduce64<WPA>(v, s, warp, lane);
+        if (tid == 0) {
+            atomicAdd(&A.F[3 * i], s.red[0]);
+            atomicAdd(&A.F[3 * i + 1], s.red[1]);
+            atomicAdd(&A.F[3 * i + 2], s.red[2]);
+            for (int k = 0; k < 6; k++) A.vir[(size_t)i * 6 + k] = s.red[3 + k];
+        }
+        for (int t = tid; t < n; t += NT) {
+            const int j = s.j[t];
+            atomicAdd(&A.F[3 * j], s.Fnb[3 * t]);
+            atomicAdd(&A.F[3 * j + 1], s.Fnb[3 * t + 1]);
+            atomicAdd(&A.F[3 * j + 2], s.Fnb[3 * t + 2]);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* reductions                                                          */
 /* ------------------------------------------------------------------ */
 
@@ -1247,6 +1941,7 @@ struct EfsShape {
 static const EfsShape kShapes[] = {{1, 4}, {4, 1}, {8, 1}};
 #define EFS_STATIC_SMEM (sizeof(mb_params) + 16) /* k_efs's __shared__ Ps, with alignment slack */
 #define MB_NSHAPES 3
+#define MB_MAX_DEVICES_K 64
 
 /* specialised kernel for the reference bases: 7 G4 exponents, 4 zeta, 2 lambda */
 static bool efs_fast(const mb_model *m) { return m->P.ne <= 7 && m->P.nz <= 4 && m->P.nlam <= 2; }
@@ -1295,11 +1990,13 @@ extern "C" int mbk_nlist(mb_dev *d, int N, int NM, const mb_cell *c, double rc, 
         k_cell_sort<<<(ncell + 127) / 128, 128, 0, st>>>(ncell, d->cell_start, d->cell_atoms);
         k_nlist_cell<<<blocks, warps_per_block * 32, 0, st>>>(N, NM, d->capNB, d->X, *c, rc2, d->cell_of,
                                                               d->cell_start, d->cell_atoms, d->nn, d->nj,
-                                                              (double4 *)d->nd, d->status);
+                                                              (double4 *)d->nd, d->status,
+                                                              d->legs_on ? d->nk : nullptr);
         *launches += 5;
     } else {
         k_nlist_brute<<<blocks, warps_per_block * 32, 0, st>>>(N, NM, d->capNB, d->X, *c, rc2, d->nn, d->nj,
-                                                               (double4 *)d->nd, d->status);
+                                                               (double4 *)d->nd, d->status,
+                                                               d->legs_on ? d->nk : nullptr);
         *launches += 1;
     }
     return (int)cudaGetLastError();
@@ -1309,14 +2006,18 @@ template <int NE, int NZ, int NLAM, int WPA, int APB>
 static int launch_shape(const EfsArgs &a, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
     auto kern = k_efs<NE, NZ, NLAM, WPA, APB>;
     size_t smem = a.smem_group * APB;
-    static size_t configured = 0;
+    /* the shared-memory opt-in is a per-device attribute of the function:
+     * remembered per device */
+    static size_t configured[MB_MAX_DEVICES_K] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MB_MAX_DEVICES_K) return (int)cudaErrorInvalidDevice;
     /* the 48 KB default and the 227 KB opt-in limit both count the kernel's
      * static shared block (the staged mb_params) as well as the dynamic part */
     if (smem + EFS_STATIC_SMEM > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
-    if (smem + EFS_STATIC_SMEM > 48 * 1024 && smem > configured) {
+    if (smem + EFS_STATIC_SMEM > 48 * 1024 && smem > configured[dev]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
-        configured = smem;
+        configured[dev] = smem;
     }
     if (e0) mbk_record(e0, st);
     kern<<<(a.N + APB - 1) / APB, WPA * 32 * APB, smem, st>>>(a);
@@ -1342,13 +2043,142 @@ static int launch_any(const mb_model *m, int shape, EfsArgs a, cudaStream_t st, 
     }
 }
 
+/* ---- leg-table path ---- */
+
+/* The leg-table path applies to the model: every forward and derivative
+ * function shares the list cutoff, the pair-mixed G4 exponents equal the
+ * species-0 ones to rounding (so one leg row serves the energy and the
+ * derivative terms), and the basis has the reference's shape (<= 8 G4
+ * exponents, <= 4 integer zeta, <= 2 lambda). */
+static bool leg_model_ok(const mb_model *m) {
+    const mb_params &P = m->P;
+    if (P.ng4 < 1 || P.ne > 8 || P.nz > 4 || P.nlam > 2 || !P.zeta_int) return false;
+    const double rc = m->rc_list;
+    if (P.d_rc2 != rc || P.d_rc4 != rc) return false;
+    for (int s = 0; s < P.nspc; s++)
+        for (int t = 0; t < P.nspc; t++) {
+            const int p = s * s + t * t;
+            if (P.f_rc2[p] != rc || P.f_rc4[p] != rc) return false;
+            for (int e = 0; e < P.ne; e++)
+                if (fabs(P.f_eta4[p][e] - P.d_eta4[e]) > 1e-12 * fabs(P.d_eta4[e])) return false;
+        }
+    return true;
+}
+
+extern "C" int mbk_legs_model(const mb_model *m) { return leg_model_ok(m) ? 1 : 0; }
+
+/* 1 when a pass of N atoms in cell c can run on leg tables: the model
+ * qualifies, the tables are allocated, and every entry key fits (atom
+ * index in 17 bits, images within +-15, neighbour capacity <= 128) */
+extern "C" int mbk_legs_usable(const mb_dev *d, const mb_model *m, int N, const mb_cell *c) {
+    if (!d->nk || !d->leg || !d->nso) return 0;
+    if (N >= MB_LEG_MAX_ATOMS || d->capNB > MB_LEG_MAX_CAP) return 0;
+    for (int q = 0; q < 3; q++)
+        if (c->Nq[q] > MB_LEG_MAX_IMAGE) return 0;
+    return leg_model_ok(m) ? 1 : 0;
+}
+
+static const EfsShape kLegShapes[] = {{1, 4}, {1, 2}, {2, 1}, {4, 1}};
+#define MB_NLEGSHAPES 4
+
+/* triplet-list entries per atom group: 1536 per warp for one warp per atom
+ * (about 930 triplets per atom in the dense alloy), 1024 per warp otherwise,
+ * never more than there are candidate pairs */
+static int tl_entries_leg(int capNB, int wpa) {
+    const int all = capNB * (capNB - 1) / 2 + 32 * wpa;
+    const int v = wpa * (wpa == 1 ? 1536 : 1024);
+    return v < all ? v : all;
+}
+
+static size_t leg_group_bytes(const mb_model *m, int capNB, int wpa) {
+    return leg_smem_bytes(capNB, m->P.D, m->P.ng2, wpa, tl_entries_leg(capNB, wpa));
+}
+
+template <int WPA, int APB>
+static int launch_leg(const LegArgs &a, cudaStream_t st) {
+    auto kern = k_efs_leg<WPA, APB>;
+    const size_t smem = a.smem_group * APB;
+    static size_t configured[MB_MAX_DEVICES_K] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MB_MAX_DEVICES_K) return (int)cudaErrorInvalidDevice;
+    if (smem + EFS_STATIC_SMEM > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
+    if (smem + EFS_STATIC_SMEM > 48 * 1024 && smem > configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        configured[dev] = smem;
+    }
+    kern<<<(a.N + APB - 1) / APB, WPA * 32 * APB, smem, st>>>(a);
+    return (int)cudaGetLastError();
+}
+
+/* k_legs then k_efs_leg in shape `shape`; the events (if any) bracket both */
+static int launch_leg_pass(const mb_dev *d, const mb_model *m, int shape, LegArgs a, cudaStream_t st, cudaEvent_t e0,
+                           cudaEvent_t e1) {
+    a.smem_group = leg_group_bytes(m, a.cap, kLegShapes[shape].wpa);
+    a.tl_cap = tl_entries_leg(a.cap, kLegShapes[shape].wpa);
+    if (e0) mbk_record(e0, st);
+    k_legs<<<(a.N + 3) / 4, 128, 0, st>>>(a.N, a.cap, d->nn, d->nj, d->nk, (double4 *)d->nd, d->spc, d->params,
+                                         d->leg, d->nso);
+    int rc;
+    switch (shape) {
+        case 0: rc = launch_leg<1, 4>(a, st); break;
+        case 1: rc = launch_leg<1, 2>(a, st); break;
+        case 2: rc = launch_leg<2, 1>(a, st); break;
+        default: rc = launch_leg<4, 1>(a, st); break;
+    }
+    if (e1) mbk_record(e1, st);
+    return rc;
+}
+
 /* Autotuner: on the first pass of a (mode, size bucket, capacity) the three
  * shapes are each timed once (after an untimed launch) and the fastest is
  * kept for later passes of that key. */
-static int tune_shape(mb_dev *d, const mb_model *m, int N, int mode, const EfsArgs &a, cudaStream_t st) {
-    int bucket = 0, k;
+static int tune_key(const mb_dev *d, int N, int mode) {
+    int bucket = 0;
     while ((1 << bucket) < N) bucket++;
-    int key = (mode << 28) | (bucket << 20) | (d->capNB & 0xfffff);
+    return (mode << 28) | ((d->legs_on ? 1 : 0) << 26) | (bucket << 20) | (d->capNB & 0xfffff);
+}
+
+static int tune_leg(mb_dev *d, const mb_model *m, int N, int mode, const LegArgs &a, cudaStream_t st) {
+    const int key = tune_key(d, N, mode);
+    for (int k = 0; k < d->tune_n; k++)
+        if (d->tune_key[k] == key) return d->tune_val[k];
+    if (d->tune_fixed >= 0) return d->tune_fixed < MB_NLEGSHAPES ? d->tune_fixed : 0;
+    LegArgs t = a;
+    t.counters = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = 0;
+    float best_ms = 1e30f;
+    for (int sh = 0; sh < MB_NLEGSHAPES; sh++) {
+        if (leg_group_bytes(m, a.cap, kLegShapes[sh].wpa) * kLegShapes[sh].apb + EFS_STATIC_SMEM > 227 * 1024) continue;
+        float ms = 1e30f;
+        int bad = 0;
+        for (int rep = 0; rep < 2 && !bad; rep++) {
+            if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
+            bad = launch_leg_pass(d, m, sh, t, st, rep ? e0 : nullptr, rep ? e1 : nullptr);
+        }
+        if (!bad && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = sh;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGetLastError();
+    if (d->tune_n < MB_TUNE_SLOTS) {
+        d->tune_key[d->tune_n] = key;
+        d->tune_val[d->tune_n] = best;
+        d->tune_n++;
+    }
+    return best;
+}
+
+static int tune_shape(mb_dev *d, const mb_model *m, int N, int mode, const EfsArgs &a, cudaStream_t st) {
+    int k;
+    const int key = tune_key(d, N, mode);
     for (k = 0; k < d->tune_n; k++)
         if (d->tune_key[k] == key) return d->tune_val[k];
     if (d->tune_fixed >= 0) return d->tune_fixed;
@@ -1407,6 +2237,42 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
     a.counters = d->counters;
     a.smem_group = 0;
     cudaMemsetAsync(d->EU, 0, sizeof(double) * N, st);
+    if (d->legs_on) {
+        LegArgs la;
+        la.N = N;
+        la.cap = d->capNB;
+        la.mode = mode;
+        la.urep = urep;
+        la.nn = d->nn;
+        la.nj = d->nj;
+        la.nso = d->nso;
+        la.nk = d->nk;
+        la.nd = (const double4 *)d->nd;
+        la.leg = d->leg;
+        la.spc = d->spc;
+        la.params = d->params;
+        la.weights = d->weights;
+        la.EA = d->EA;
+        la.EU = d->EU;
+        la.G = d->G;
+        la.F = d->F;
+        la.vir = d->vir;
+        la.counters = d->counters;
+        la.smem_group = 0;
+        la.tl_cap = 0;
+        const int shape = tune_leg(d, m, N, mode, la, st);
+        d->last_shape = 16 + shape;
+        cudaEvent_t e0 = 0, e1 = 0;
+        if (d->ev_on && d->ev_n < d->ev_cap) {
+            e0 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n];
+            e1 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n + 1];
+            d->ev_n++;
+        }
+        if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
+        const int rc = launch_leg_pass(d, m, shape, la, st, e0, e1);
+        (*launches) += 2;
+        return rc;
+    }
     int shape = tune_shape(d, m, N, mode, a, st);
     d->last_shape = shape;
     cudaEvent_t e0 = 0, e1 = 0;
@@ -1458,10 +2324,9 @@ extern "C" void mbk_record(void *event, void *stream) {
 /* 1 when the descriptor pass of (N, mode) at the current capacity has its
  * kernel shape already: only then may it be captured (tuning synchronises) */
 extern "C" int mbk_shape_ready(const mb_dev *d, int N, int mode) {
-    int bucket = 0, k;
+    int k;
     if (d->tune_fixed >= 0) return 1;
-    while ((1 << bucket) < N) bucket++;
-    const int key = (mode << 28) | (bucket << 20) | (d->capNB & 0xfffff);
+    const int key = tune_key(d, N, mode);
     for (k = 0; k < d->tune_n; k++)
         if (d->tune_key[k] == key) return 1;
     return 0;

@@ -20,11 +20,15 @@ int mb_handle_device(const mb_potential *p);
 int mb_handle_fail(int code, const char *msg);
 void mb_handle_set_batch_stats(mb_potential *p, long long evals, float ms);
 
-int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, double *lat, double *x, double p_gpa,
-                   double urep, int rlxt, int mitr, double fmax, double *H, int *iters, int *status) {
+/* The population relax and the batched E/F/S share this: with frc/str set
+ * the kernel also returns each structure's forces and virial at its final
+ * state, and with keep_xyz = 0 the positions and lattices are not copied back. */
+static int batch_run(mb_potential *pot, int S, const int *nat, const int *atmn, double *lat, double *x, double p_gpa,
+                     double urep, int rlxt, int mitr, double fmax, double *H, int *iters, int *status, double *frc,
+                     double *str, int keep_xyz) {
     int *off, *order, total = 0, s, rc = MB_OK;
     int *d_nat = NULL, *d_off = NULL, *d_spc = NULL, *d_iters = NULL, *d_status = NULL, *d_order = NULL;
-    double *d_lat = NULL, *d_x = NULL, *d_H = NULL;
+    double *d_lat = NULL, *d_x = NULL, *d_H = NULL, *d_frc = NULL, *d_str = NULL;
     long long evals = 0;
     float ms = 0.0f;
     const mb_model *m;
@@ -69,6 +73,8 @@ int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, do
     if (!e) e = cudaMalloc((void **)&d_x, sizeof(double) * 3 * total);
     if (!e) e = cudaMalloc((void **)&d_H, sizeof(double) * S);
     if (!e) e = cudaMalloc((void **)&d_order, sizeof(int) * S);
+    if (!e && frc) e = cudaMalloc((void **)&d_frc, sizeof(double) * 3 * total);
+    if (!e && str) e = cudaMalloc((void **)&d_str, sizeof(double) * 6 * S);
     if (!e) e = cudaMemcpyAsync(d_order, order, sizeof(int) * S, cudaMemcpyHostToDevice, (cudaStream_t)st);
     if (!e) e = cudaMemcpyAsync(d_nat, nat, sizeof(int) * S, cudaMemcpyHostToDevice, (cudaStream_t)st);
     if (!e) e = cudaMemcpyAsync(d_off, off, sizeof(int) * (S + 1), cudaMemcpyHostToDevice, (cudaStream_t)st);
@@ -80,7 +86,8 @@ int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, do
         goto out;
     }
     e = (cudaError_t)mbk_relax_batch(m, S, d_nat, d_off, d_spc, d_order, d_lat, d_x, p_gpa / MB_EV2GPA, urep > 0 ? urep : 0.0,
-                                     rlxt, mitr, fmax, d_H, d_iters, d_status, st, &evals, &ms);
+                                     rlxt, mitr, fmax, d_H, d_iters, d_status, frc ? d_frc : NULL,
+                                     frc ? d_str : NULL, st, &evals, &ms);
     if (e == cudaErrorInvalidValue) {
         rc = mb_handle_fail(MB_ERR_MODEL, "batched relax needs a basis with <= 7 G4 exponents, zeta in {integers}, "
                                           "2 lambdas, <= 16 G2 functions and D <= 288");
@@ -90,8 +97,13 @@ int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, do
         rc = mb_handle_fail(MB_ERR_CUDA, cudaGetErrorString(e));
         goto out;
     }
-    e = cudaMemcpy(lat, d_lat, sizeof(double) * 9 * S, cudaMemcpyDeviceToHost);
-    if (!e) e = cudaMemcpy(x, d_x, sizeof(double) * 3 * total, cudaMemcpyDeviceToHost);
+    e = cudaSuccess;
+    if (keep_xyz) {
+        e = cudaMemcpy(lat, d_lat, sizeof(double) * 9 * S, cudaMemcpyDeviceToHost);
+        if (!e) e = cudaMemcpy(x, d_x, sizeof(double) * 3 * total, cudaMemcpyDeviceToHost);
+    }
+    if (!e && frc) e = cudaMemcpy(frc, d_frc, sizeof(double) * 3 * total, cudaMemcpyDeviceToHost);
+    if (!e && frc && str) e = cudaMemcpy(str, d_str, sizeof(double) * 6 * S, cudaMemcpyDeviceToHost);
     if (!e) e = cudaMemcpy(H, d_H, sizeof(double) * S, cudaMemcpyDeviceToHost);
     if (!e) e = cudaMemcpy(iters, d_iters, sizeof(int) * S, cudaMemcpyDeviceToHost);
     if (!e) e = cudaMemcpy(status, d_status, sizeof(int) * S, cudaMemcpyDeviceToHost);
@@ -99,8 +111,72 @@ int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, do
     mb_handle_set_batch_stats(pot, evals, ms);
 out:
     cudaFree(d_nat); cudaFree(d_off); cudaFree(d_spc); cudaFree(d_iters); cudaFree(d_status);
-    cudaFree(d_lat); cudaFree(d_x); cudaFree(d_H); cudaFree(d_order);
+    cudaFree(d_lat); cudaFree(d_x); cudaFree(d_H); cudaFree(d_order); cudaFree(d_frc); cudaFree(d_str);
     free(off);
     free(order);
+    return rc;
+}
+
+int mb_relax_batch(mb_potential *pot, int S, const int *nat, const int *atmn, double *lat, double *x, double p_gpa,
+                   double urep, int rlxt, int mitr, double fmax, double *H, int *iters, int *status) {
+    return batch_run(pot, S, nat, atmn, lat, x, p_gpa, urep, rlxt, mitr, fmax, H, iters, status, NULL, NULL, 1);
+}
+
+int mb_efs_batch(mb_potential *pot, int S, const int *nat, const int *atmn, const double *lat, const double *x,
+                 double p_gpa, double urep, double *H, double *frc, double *str) {
+    int *iters, *status, rc;
+    if (!frc || !H || S < 1) return mb_handle_fail(MB_ERR_ARG, "bad arguments");
+    iters = (int *)malloc(sizeof(int) * S);
+    status = (int *)malloc(sizeof(int) * S);
+    /* no iterations: the kernel evaluates each structure once; the
+     * positions and lattices are read, not written back */
+    rc = batch_run(pot, S, nat, atmn, (double *)lat, (double *)x, p_gpa, urep, 3, 0, 1.0, H, iters, status, frc, str,
+                   0);
+    if (!rc)
+        for (int s = 0; s < S; s++)
+            if (status[s] == 2) {
+                rc = mb_handle_fail(MB_ERR_NEIGHBOURS, "a structure has more than 96 neighbours per atom");
+                break;
+            }
+    free(iters);
+    free(status);
+    return rc;
+}
+
+int mb_evos_write(const char *evos_dir, int gen, int member, int N, int nspc, const int *spcz, const int *atmn,
+                  const double *lat0, const double *x0, const double *lat, const double *x, double H, double E,
+                  double p_gpa, const double *frc, const double *str, int iters);
+
+int mb_evos_relax(mb_potential *pot, const char *evos_dir, int gen, int p0, int S, const int *nat, const int *atmn,
+                  double *lat, double *x, double p_gpa, double urep, int rlxt, int mitr, double fmax, double *H,
+                  int *iters, int *status) {
+    const mb_model *m;
+    double *lat0, *x0, *frc, *str;
+    int total = 0, s, rc, off = 0;
+    if (!pot || !evos_dir || S < 1 || !nat || !atmn || !lat || !x || !H || !iters || !status || p0 < 0 || gen < 0)
+        return mb_handle_fail(MB_ERR_ARG, "bad arguments");
+    for (s = 0; s < S; s++) total += nat[s] > 0 ? nat[s] : 0;
+    m = mb_handle_model(pot);
+    lat0 = (double *)malloc(sizeof(double) * 9 * S);
+    x0 = (double *)malloc(sizeof(double) * 3 * total);
+    frc = (double *)malloc(sizeof(double) * 3 * total);
+    str = (double *)malloc(sizeof(double) * 6 * S);
+    if (!lat0 || !x0 || !frc || !str) {
+        free(lat0); free(x0); free(frc); free(str);
+        return mb_handle_fail(MB_ERR_ARG, "out of memory");
+    }
+    memcpy(lat0, lat, sizeof(double) * 9 * S);
+    memcpy(x0, x, sizeof(double) * 3 * total);
+    rc = batch_run(pot, S, nat, atmn, lat, x, p_gpa, urep, rlxt, mitr, fmax, H, iters, status, frc, str, 1);
+    for (s = 0; s < S && rc == MB_OK; s++) {
+        const double *L = lat + 9 * s;
+        const double V = fabs(L[0] * L[4] * L[8] + L[2] * L[3] * L[7] + L[1] * L[5] * L[6] - L[0] * L[5] * L[7] -
+                              L[1] * L[3] * L[8] - L[2] * L[4] * L[6]);
+        const double E = H[s] - p_gpa / MB_EV2GPA * V;
+        rc = mb_evos_write(evos_dir, gen, p0 + s, nat[s], m->nspc, m->spcz, atmn + off, lat0 + 9 * s, x0 + 3 * off,
+                           L, x + 3 * off, H[s], E, p_gpa, frc + 3 * off, str + 6 * s, iters[s]);
+        off += nat[s];
+    }
+    free(lat0); free(x0); free(frc); free(str);
     return rc;
 }

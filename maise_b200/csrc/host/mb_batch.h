@@ -7,7 +7,7 @@ extern "C" {
 #endif
 int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const int *d_off, const int *d_spc,
                     const int *d_order, double *d_lat, double *d_x, double p_ev, double urep, int rlxt, int mitr, double fmax, double *d_H, int *d_iters,
-                    int *d_status, void *stream, long long *evals_out, float *ms_out);
+                    int *d_status, double *d_frc, double *d_str, void *stream, long long *evals_out, float *ms_out);
 #ifdef __cplusplus
 }
 #endif

@@ -26,7 +26,7 @@
  * of this is unchanged (buffers, sizes, step parameters, profiling state) */
 typedef struct {
     long gen;
-    int N, NM, chunk, st_on, ev_on;
+    int N, NM, chunk, st_on, ev_on, legs;
     double urep, dt, tau, T;
     mb_cell c;
     void *flush, *trace, *st_pool, *ev_pool;
@@ -36,7 +36,7 @@ typedef struct {
 /* what a single-structure pass graph was captured for */
 typedef struct {
     long gen;
-    int N, NM, ND, mode, M[3];
+    int N, NM, ND, mode, M[3], legs;
     double urep;
     void *h_res;
 } pass_key;
@@ -70,6 +70,9 @@ struct mb_potential {
     size_t h_buf_len;
     int *h_status;
     double *h_out;
+    /* leg tables for the descriptor pass: the model qualifies and they are
+     * not switched off (MAISE_B200_LEGS=0) */
+    int legs_enabled;
     /* MD chunk graph */
     int use_graphs;
     cudaGraphExec_t md_exec;
@@ -142,6 +145,10 @@ int mb_open(const char *model_path, int device, mb_potential **out) {
         const char *fx = getenv("MAISE_B200_SHAPE");
         if (fx) p->d.tune_fixed = atoi(fx);
     }
+    {
+        const char *lg = getenv("MAISE_B200_LEGS");
+        p->legs_enabled = mbk_legs_model(&p->m) && !(lg && lg[0] == '0');
+    }
     CK(cudaSetDevice(device), "cudaSetDevice");
     CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     CK(cudaMalloc((void **)&p->d.params, sizeof(mb_params)), "cudaMalloc params");
@@ -165,6 +172,7 @@ int mb_open(const char *model_path, int device, mb_potential **out) {
 }
 
 static void dev_free(mb_dev *d) {
+    cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso);
     cudaFree(d->X); cudaFree(d->V); cudaFree(d->spc); cudaFree(d->nn); cudaFree(d->nj); cudaFree(d->nd);
     cudaFree(d->F); cudaFree(d->EA); cudaFree(d->EU); cudaFree(d->vir); cudaFree(d->G);
     cudaFree(d->cell_of); cudaFree(d->cell_cnt); cudaFree(d->cell_start); cudaFree(d->cell_atoms);
@@ -365,16 +373,23 @@ static int ensure(mb_potential *p, int N, int nb, int ncell) {
         CK(cudaMalloc((void **)&d->cell_atoms, sizeof(int) * cap), "alloc cell_atoms");
         d->capN = cap;
         p->gen++;
-        cudaFree(d->nj); cudaFree(d->nd);
-        d->nj = NULL; d->nd = NULL;
+        cudaFree(d->nj); cudaFree(d->nd); cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso);
+        d->nj = NULL; d->nd = NULL; d->nk = NULL; d->leg = NULL; d->nso = NULL;
         d->capNB = 0;
     }
     if (nb > d->capNB || !d->nj) {
         int cap = nb > d->capNB ? nb : d->capNB;
         cap = (cap + 7) & ~7;
-        cudaFree(d->nj); cudaFree(d->nd);
+        cudaFree(d->nj); cudaFree(d->nd); cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso);
+        d->nk = NULL; d->leg = NULL; d->nso = NULL;
         CK(cudaMalloc((void **)&d->nj, sizeof(int) * (size_t)cap * d->capN), "alloc nj");
         CK(cudaMalloc((void **)&d->nd, sizeof(double) * 4 * (size_t)cap * d->capN), "alloc nd");
+        if (p->legs_enabled && cap <= MB_LEG_MAX_CAP) {
+            /* leg tables of the descriptor pass (the model qualifies for them) */
+            CK(cudaMalloc((void **)&d->nk, sizeof(unsigned) * (size_t)cap * d->capN), "alloc nk");
+            CK(cudaMalloc((void **)&d->leg, sizeof(double) * MB_LEG_STRIDE * (size_t)cap * d->capN), "alloc legs");
+            CK(cudaMalloc((void **)&d->nso, sizeof(int) * 4 * (size_t)d->capN), "alloc nso");
+        }
         d->capNB = cap;
         p->gen++;
     }
@@ -433,7 +448,11 @@ static double cell_volume(const double *L) {
     return fabs(V);
 }
 
-static void setup_cell(const mb_potential *p, const double *lat9, int ND, int N, mb_cell *c) {
+/* bins: 0 as the passes choose (cell list for N >= 64 when every periodic
+ * direction holds >= 3 bins no thinner than Rc and there are >= 8 bins),
+ * 1 never (all-pairs search), 2 whenever the bins are valid (periodic
+ * directions >= 3 bins), whatever N */
+static void setup_cell_bins(const mb_potential *p, const double *lat9, int ND, int N, mb_cell *c, int bins) {
     double rc = p->m.rc_list;
     int q;
     memset(c, 0, sizeof(*c));
@@ -445,8 +464,8 @@ static void setup_cell(const mb_potential *p, const double *lat9, int ND, int N,
         c->Nq[q] = q < ND ? (int)ceil(rc * len) : 0;
     }
     /* bins no thinner than Rc; periodic directions need at least 3 */
-    {
-        int M[3], ok = N >= 64, total;
+    if (bins != 1) {
+        int M[3], ok = bins == 2 || N >= 64, total;
         for (q = 0; q < 3; q++) {
             double len = sqrt(c->R[3 * q] * c->R[3 * q] + c->R[3 * q + 1] * c->R[3 * q + 1] +
                               c->R[3 * q + 2] * c->R[3 * q + 2]);
@@ -457,9 +476,13 @@ static void setup_cell(const mb_potential *p, const double *lat9, int ND, int N,
             if (q < ND && M[q] < 3) ok = 0;
         }
         total = M[0] * M[1] * M[2];
-        if (ok && total >= 8)
+        if (ok && (bins == 2 || total >= 8))
             for (q = 0; q < 3; q++) c->M[q] = M[q];
     }
+}
+
+static void setup_cell(const mb_potential *p, const double *lat9, int ND, int N, mb_cell *c) {
+    setup_cell_bins(p, lat9, ND, N, c, 0);
 }
 
 /* accessors used by mb_static.cu */
@@ -568,6 +591,7 @@ static int graph_pass(mb_potential *p, int N, int NM, int ND, const mb_cell *c, 
     k.M[2] = c->M[2];
     k.urep = urep;
     k.h_res = p->h_res;
+    k.legs = p->d.legs_on;
     if (!q->x || memcmp(&k, &q->k, sizeof(k))) {
         cudaGraph_t g = NULL;
         if (!q->seen_valid || memcmp(&k, &q->seen, sizeof(k))) {
@@ -628,6 +652,7 @@ static int run_pass(mb_potential *p, int N, int NM, int ND, const double *lat9, 
     if (ND == 3) pV = p_gpa / MB_EV2GPA * cell_volume(lat9);
     ncell = c.M[0] ? c.M[0] * c.M[1] * c.M[2] : 1;
     if ((r = ensure(p, N, p->d.capNB ? p->d.capNB : (NM < 64 ? NM : 64), ncell))) return r;
+    p->d.legs_on = mbk_legs_usable(&p->d, &p->m, N, &c);
     p->res_staged = 0;
     r = MB_FALLBACK;
     if (p->use_graphs && !p->pbroken && !p->d.ev_on && mbk_shape_ready(&p->d, N, mode)) {
@@ -723,6 +748,77 @@ int mb_descriptor_vjp(mb_potential *p, int N, int NM, int ND, int XT, const int 
     if (frc) CK(cudaMemcpyAsync(frc, p->d.F, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, p->stream), "D2H forces");
     CK(cudaStreamSynchronize(p->stream), "synchronize");
     return MB_OK;
+}
+
+int mb_neighbours(mb_potential *p, int N, int NM, int ND, int XT, const int *atmn, const double *lat9, const double *x,
+                  int path, int cap, int *nn, int *nj, int *shift, double *x_wrapped) {
+    mb_cell c;
+    int r, tries, i, t, q, ncell, capNB;
+    int *hnn = NULL, *hnj = NULL;
+    double *hnd = NULL, *hx = NULL;
+    if (!p || N < 1 || NM < 1 || ND < 0 || ND > 3 || !atmn || !lat9 || !x || cap < 1 || !nn || !nj || !shift ||
+        path < 0 || path > 2)
+        return fail(MB_ERR_ARG, "bad arguments");
+    CK(cudaSetDevice(p->device), "cudaSetDevice");
+    setup_cell_bins(p, lat9, ND, N, &c, path);
+    if (path == 2 && !c.M[0]) return fail(MB_ERR_ARG, "the cell cannot be binned (a periodic direction is under 3 Rc wide)");
+    ncell = c.M[0] ? c.M[0] * c.M[1] * c.M[2] : 1;
+    if ((r = ensure(p, N, p->d.capNB ? p->d.capNB : (NM < 64 ? NM : 64), ncell))) return r;
+    p->d.legs_on = 0;
+    for (tries = 0; tries < 3; tries++) {
+        if ((r = upload(p, N, XT, atmn, lat9, x))) return r;
+        CK(cudaMemsetAsync(p->d.status, 0, sizeof(int) * 4, p->stream), "memset status");
+        if ((r = mbk_wrap(&p->d, N, &c, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "wrap");
+        if ((r = mbk_nlist(&p->d, N, NM, &c, p->m.rc_list, p->stream, &p->launches)))
+            return cuda_fail((cudaError_t)r, "neighbour list");
+        CK(cudaMemcpyAsync(p->h_status, p->d.status, sizeof(int) * 4, cudaMemcpyDeviceToHost, p->stream), "D2H status");
+        CK(cudaStreamSynchronize(p->stream), "synchronize");
+        if (p->h_status[0] & MB_ST_WRAP) return fail(MB_ERR_STATE, "non-finite or runaway positions");
+        if (p->h_status[0] & MB_ST_NBR_OVERFLOW)
+            return fail(MB_ERR_NEIGHBOURS, "an atom reached NM=%d neighbours within %.4f A; increase NM", NM, p->m.rc_list);
+        if (!(p->h_status[0] & MB_ST_CAP_OVERFLOW)) break;
+        if ((r = ensure(p, N, p->h_status[1] + 8, ncell))) return r;
+    }
+    if (tries == 3) return fail(MB_ERR_CAPACITY, "neighbour capacity could not be established");
+    if (p->h_status[1] > cap) return fail(MB_ERR_CAPACITY, "an atom has %d neighbours; cap is %d", p->h_status[1], cap);
+    capNB = p->d.capNB;
+    hnn = (int *)malloc(sizeof(int) * N);
+    hnj = (int *)malloc(sizeof(int) * (size_t)N * capNB);
+    hnd = (double *)malloc(sizeof(double) * 4 * (size_t)N * capNB);
+    hx = (double *)malloc(sizeof(double) * 3 * N);
+    if (!hnn || !hnj || !hnd || !hx) {
+        r = fail(MB_ERR_ARG, "out of host memory");
+        goto out;
+    }
+    if (cudaMemcpy(hnn, p->d.nn, sizeof(int) * N, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(hnj, p->d.nj, sizeof(int) * (size_t)N * capNB, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(hnd, p->d.nd, sizeof(double) * 4 * (size_t)N * capNB, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(hx, p->d.X, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        r = fail(MB_ERR_CUDA, "D2H neighbour list");
+        goto out;
+    }
+    /* the kernels keep each entry's displacement d = S + (x_j - x_i) with
+     * S = sum_q ic_q L_q; ic_q = rint(S . R_q) since L_p . R_q = delta_pq */
+    for (i = 0; i < N; i++) {
+        nn[i] = hnn[i];
+        for (t = 0; t < hnn[i]; t++) {
+            const size_t o = (size_t)i * capNB + t, w = (size_t)i * cap + t;
+            const int j = hnj[o];
+            double S[3];
+            nj[w] = j;
+            for (q = 0; q < 3; q++) S[q] = hnd[4 * o + q] - (hx[3 * j + q] - hx[3 * i + q]);
+            for (q = 0; q < 3; q++)
+                shift[3 * w + q] = (int)lrint(S[0] * c.R[3 * q] + S[1] * c.R[3 * q + 1] + S[2] * c.R[3 * q + 2]);
+        }
+    }
+    if (x_wrapped) memcpy(x_wrapped, hx, sizeof(double) * 3 * N);
+    r = MB_OK;
+out:
+    free(hnn);
+    free(hnj);
+    free(hnd);
+    free(hx);
+    return r;
 }
 
 /* ------------------------------------------------------------------ */
@@ -1023,6 +1119,7 @@ static int md_chunk(mb_potential *p, int N, int NM, const mb_cell *c, double ure
                     int step, int chunk, int *graphed) {
     int r, s;
     *graphed = 0;
+    p->d.legs_on = mbk_legs_usable(&p->d, &p->m, N, c);
     CK(cudaMemsetAsync(p->d.status, 0, sizeof(int) * 4, p->stream), "memset status");
     if ((r = mbk_set_out(&p->d, 10, (double)step, p->stream))) return cuda_fail((cudaError_t)r, "set step");
     if (p->use_graphs && mbk_shape_ready(&p->d, N, MB_MODE_EFS)) {
@@ -1044,6 +1141,7 @@ static int md_chunk(mb_potential *p, int N, int NM, const mb_cell *c, double ure
         k.trace = p->d.trace;
         k.st_pool = p->d.st_pool;
         k.ev_pool = p->d.ev_pool;
+        k.legs = p->d.legs_on;
         if (!p->md_exec || memcmp(&k, &p->md_k, sizeof(k))) {
             cudaGraph_t g = NULL;
             cudaError_t e;

@@ -82,6 +82,13 @@ typedef struct {
     int M[3];      /* cell-list bins per direction (0: brute force) */
 } mb_cell;
 
+/* leg-table path of the descriptor pass: one row per neighbour-list entry,
+ * exp(-eta_e r^2) for e < 8, fc(r), fc'(r)/r */
+#define MB_LEG_STRIDE 10
+#define MB_LEG_MAX_ATOMS (1 << 17) /* atom index in 17 bits of an entry key */
+#define MB_LEG_MAX_IMAGE 15        /* |image| per axis in 5 bits of an entry key */
+#define MB_LEG_MAX_CAP 128         /* neighbour capacity the leg kernels handle */
+
 /* status bits written by kernels */
 #define MB_ST_NBR_OVERFLOW 1   /* an atom reached NM neighbours */
 #define MB_ST_CAP_OVERFLOW 2   /* more neighbours than device capacity */
@@ -118,6 +125,15 @@ typedef struct {
     unsigned long long *counters; /* [2]: pairs and triplets seen by the descriptor kernel */
     mb_params *params;
     double *weights;
+    /* leg tables (see mb_kernels.cu, k_legs): with legs_on the list kernels
+     * also write each entry's key (atom << 15 | image, 5 bits per axis),
+     * k_legs sorts every atom's list by species (nso[4N]: species starts
+     * and the count) and fills leg[N*capNB*MB_LEG_STRIDE] with each entry's
+     * exp(-eta_e r^2), fc(r) and fc'(r)/r; NULL where not allocated */
+    unsigned *nk;
+    double *leg;
+    int *nso;
+    int legs_on;
     /* optional CUDA-event timing of the descriptor kernel */
     int ev_on, ev_n, ev_cap;
     void *ev_pool;    /* cudaEvent_t[2*ev_cap] */
@@ -144,6 +160,8 @@ int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, d
 int mbk_set_out(mb_dev *d, int idx, double v, void *stream);
 void mbk_record(void *event, void *stream);
 int mbk_shape_ready(const mb_dev *d, int N, int mode);
+int mbk_legs_model(const mb_model *m);
+int mbk_legs_usable(const mb_dev *d, const mb_model *m, int N, const mb_cell *c);
 int mbk_graph_cell_nodes(void *graph, void **nodes, int *rows, int cap);
 int mbk_graph_set_cell(void *exec, void *const *nodes, const int *rows, int count, const mb_cell *c, double pV);
 size_t mbk_efs_smem(const mb_model *m, int capNB, int shape);

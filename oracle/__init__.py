@@ -39,12 +39,24 @@ def _ip(a):
     return a.ctypes.data_as(_I)
 
 
+# Where the build recipe looks for the reference MAISE sources: the
+# MAISE_REFERENCE environment variable, else the read-only mount point of the
+# build container.  Nothing at test or benchmark time reads the sources.
+_REFERENCE_MOUNT = "/root/reference"
+
+
+def reference_dir():
+    """Directory of the reference sources for the build recipe, or None."""
+    d = os.environ.get("MAISE_REFERENCE") or _REFERENCE_MOUNT
+    return d if os.path.isdir(os.path.join(d, "src")) else None
+
+
 def build(ref: bool = True) -> None:
     """Compile the restatement (and the reference, when its sources exist)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and os.path.isdir(os.environ.get("MAISE_REFERENCE", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8",
-                        "REF=" + os.environ.get("MAISE_REFERENCE", "/root/reference")], check=True)
+    src = reference_dir() if ref else None
+    if src:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8", "REF=" + src], check=True)
 
 
 def ref_available() -> bool:
@@ -190,9 +202,14 @@ class RefOracle:
             lib.ref_relax.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _L]
             lib.ref_nvt.restype = c_d
             lib.ref_nvt.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, _D, c_i, ctypes.c_long, c_d,
-                                    c_d, c_d, c_i, c_d, _D, _D]
+                                    c_d, c_d, c_i, c_d, _D, _D, c_d]
             lib.ref_maxwell.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, ctypes.c_long, c_d, _D]
             lib.ref_sizes.argtypes = [_I]
+            lib.ref_nlist.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, c_i, _I, _I, _I, _D]
+            lib.ref_read_cell.argtypes = [ctypes.c_char_p, c_i, _I, _D, _D, _I]
+            lib.ref_read_oszi.restype = c_d
+            lib.ref_rdf.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_d, c_i, _D]
+            lib.ref_read_oszi.argtypes = [ctypes.c_char_p]
             cls._lib = lib
         return cls._lib
 
@@ -242,7 +259,7 @@ class RefOracle:
         return dict(H=H, X=X.reshape(-1, 3), LAT=LAT.reshape(3, 3), n_energy=int(counts[0]),
                     n_force=int(counts[1]), iters=int(counts[2]))
 
-    def nvt(self, X, LAT, atmn, ND, T, dt, tau, nsteps, seed=1, V=None, urep=0.0, NM=512):
+    def nvt(self, X, LAT, atmn, ND, T, dt, tau, nsteps, seed=1, V=None, urep=0.0, NM=512, xi=0.0):
         X, LAT, atmn = Oracle._prep(X, LAT, atmn)
         N = len(atmn)
         vin = V is not None
@@ -250,8 +267,48 @@ class RefOracle:
         Hs = np.zeros(nsteps)
         Ks = np.zeros(nsteps)
         xi = self.lib().ref_nvt(self.dir, N, NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), _dp(V), int(vin),
-                                seed, T, dt, tau, nsteps, urep, _dp(Hs), _dp(Ks))
+                                seed, T, dt, tau, nsteps, urep, _dp(Hs), _dp(Ks), xi)
         return dict(X=X.reshape(N, 3), V=V.reshape(N, 3), H=Hs, K=Ks, xi=xi)
+
+    def nlist(self, X, LAT, atmn, ND, NM=512, cap=None):
+        """LIST's neighbour list: (nn[N], nj[N,cap], nic[N,cap,3] integer images, X wrapped)."""
+        X, LAT, atmn = Oracle._prep(X, LAT, atmn)
+        N = len(atmn)
+        cap = cap or NM
+        nn = np.zeros(N, np.int32)
+        nj = np.zeros(N * cap, np.int32)
+        nic = np.zeros(N * cap * 3, np.int32)
+        Xw = np.zeros(3 * N)
+        if self.lib().ref_nlist(self.dir, N, NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), cap, _ip(nn), _ip(nj),
+                                _ip(nic), _dp(Xw)):
+            raise RuntimeError("more neighbours than cap")
+        return nn, nj.reshape(N, cap), nic.reshape(N, cap, 3), Xw.reshape(N, 3)
+
+    def read_cell(self, path, cap=4096):
+        """READ_CELL of a POSCAR/CONTCAR (a model must have been loaded by an
+        earlier call): dict(LAT[3,3], X[N,3] Cartesian, atmn[N])."""
+        N = ctypes.c_int()
+        lat = np.zeros(9)
+        X = np.zeros(3 * cap)
+        atmn = np.zeros(cap, np.int32)
+        rv = self.lib().ref_read_cell(os.fsencode(path), cap, ctypes.byref(N), _dp(lat), _dp(X), _ip(atmn))
+        if rv:
+            raise RuntimeError(f"READ_CELL failed on {path} ({rv})")
+        n = N.value
+        return dict(LAT=lat.reshape(3, 3), X=X[: 3 * n].reshape(n, 3), atmn=atmn[:n].copy())
+
+    def rdf(self, X, LAT, atmn, ND, nspc, rmin=5.8, rmax=6.0, sigma=0.008, normalise=True, NM=512):
+        """RDF of RANK_TR's duplicate test: [npair, 3000] for species pairs m <= n."""
+        X, LAT, atmn = Oracle._prep(X, LAT, atmn)
+        npair = nspc * (nspc + 1) // 2
+        out = np.zeros(npair * 3000)
+        nb = self.lib().ref_rdf(self.dir, len(atmn), NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), rmin, rmax,
+                                sigma, int(normalise), _dp(out))
+        return out.reshape(npair, nb)
+
+    def read_oszi(self, path):
+        """The enthalpy Read_OSZI takes from an OSZICAR."""
+        return float(self.lib().ref_read_oszi(os.fsencode(path)))
 
     def maxwell(self, X, LAT, atmn, ND, T, seed=1, NM=512):
         X, LAT, atmn = Oracle._prep(X, LAT, atmn)

@@ -141,6 +141,48 @@ int ref_descriptors(const char *dir, int N, int NM, int ND, int NP, int *ATMN, d
     return hP.D;
 }
 
+/* The neighbour list of the reference's LIST (src/cell.c:82-185) for
+ * Cartesian X: nn[N] counts, and per entry t of atom i the neighbour atom
+ * nj[i*cap+t] and its integer image nic[(i*cap+t)*3+q].  LIST stores the
+ * image as the Cartesian shift S = sum_q ic_q L_q (src/cell.c:127-131);
+ * ic_q = rint(S . R_q) recovers the integers (R_q are the reciprocal rows
+ * Reciprocal() set, L_p . R_q = delta_pq).  Xw[3N] receives the positions
+ * after LIST's wrap.  Returns -1 if an atom has more than cap neighbours. */
+int ref_nlist(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *LAT, double *X, int cap, int *nn,
+              int *nj, int *nic, double *Xw) {
+    double *F = (double *)malloc(sizeof(double) * 3 * N), S[6];
+    double *Xc = (double *)malloc(sizeof(double) * 3 * N);
+    int i, t, q, rv = 0;
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    if (!h_ready || strcmp(dir, h_dir) != 0 || N > h_capN || NM != h_capNM)
+        h_call(dir, N, NM, ND, NP, 1, ATMN, LAT, Xc, F, S, 0.0, 0.0);
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    h_prologue(N, NM, ND, NP, 0.0, 0.0);
+    CAST_CELL(&hC, ATMN, LAT, Xc);
+    LIST(&hC, 0);
+    for (i = 0; i < N && !rv; i++) {
+        nn[i] = hC.Nn[i];
+        if (nn[i] > cap) {
+            rv = -1;
+            break;
+        }
+        for (t = 0; t < nn[i]; t++) {
+            size_t o = (size_t)i * cap + t;
+            nj[o] = hC.Ni[i][t];
+            for (q = 0; q < 3; q++) {
+                double s = hC.S[i][t][0] * hC.R[q][0] + hC.S[i][t][1] * hC.R[q][1] + hC.S[i][t][2] * hC.R[q][2];
+                nic[3 * o + q] = (int)lrint(s);
+            }
+        }
+    }
+    if (Xw)
+        for (i = 0; i < N; i++)
+            for (q = 0; q < 3; q++) Xw[3 * i + q] = hC.X[i][q];
+    free(F);
+    free(Xc);
+    return rv;
+}
+
 /* Derivative blocks of one atom from the last ref_descriptors call, in the
  * parse-file layout: fn[(slot*D+m)*3+q], slot == dnn is the self block. */
 int ref_fn(int atom, int *dnn, int *dni, double *fn, double *sn) {
@@ -212,14 +254,16 @@ double ref_relax(const char *dir, int N, int NM, int ND, int NP, int *ATMN, doub
  *   E+F+S, K, xi += dt/tau^2 (2K/(3 N T) - 1), x += v dt + f dt^2/2,
  *   v += f dt with f = F/m - xi v, wrap.
  * If V is non-NULL and vin != 0 the given velocities are used instead of
- * Maxwell's.  Hs[n], Ks[n] record H and K at the start of step n.  On
- * return X and V hold the final state.  Returns the final xi. */
+ * Maxwell's.  Hs[n], Ks[n] record H and K at the start of step n.  xi0 is
+ * the thermostat variable at the start (0 for a new run).  On return X and
+ * V hold the final state.  Returns the final xi. */
 double ref_nvt(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *LAT, double *X, double *V, int vin,
-               long seed, double T0, double dt, double tau, int nsteps, double urep, double *Hs, double *Ks) {
+               long seed, double T0, double dt, double tau, int nsteps, double urep, double *Hs, double *Ks,
+               double xi0) {
     double *F = (double *)malloc(sizeof(double) * 3 * N), S[6];
     double *Xc = (double *)malloc(sizeof(double) * 3 * N);
     const double kbinv = 11604.0; /* src/cmod.c:5 */
-    double T = T0 / kbinv, xi = 0.0;
+    double T = T0 / kbinv, xi = xi0;
     int i, q, n;
     memcpy(Xc, X, sizeof(double) * 3 * N);
     if (!h_ready || strcmp(dir, h_dir) != 0 || N > h_capN || NM != h_capNM)
@@ -284,4 +328,59 @@ int ref_maxwell(const char *dir, int N, int NM, int ND, int NP, int *ATMN, doubl
     free(F);
     free(Xc);
     return 0;
+}
+
+/* A POSCAR/CONTCAR read by the reference's READ_CELL (src/util.c:820-989)
+ * into the harness cell (a model must be loaded, and the file's species must
+ * be among its species): N, lattice rows, Cartesian positions and species
+ * indices.  Returns 0, -1 if the file cannot be read, -2 if N > cap. */
+int ref_read_cell(const char *path, int cap, int *N, double *lat, double *X, int *atmn) {
+    int i, q;
+    if (!h_ready) return -1;
+    hC.A = h_capN;
+    if (!READ_CELL(&hC, (char *)path)) return -1;
+    *N = hC.N;
+    if (hC.N > cap) return -2;
+    for (i = 0; i < 3; i++)
+        for (q = 0; q < 3; q++) lat[3 * i + q] = hC.L[i][q];
+    for (i = 0; i < hC.N; i++) {
+        atmn[i] = hC.ATMN[i];
+        for (q = 0; q < 3; q++) X[3 * i + q] = hC.X[i][q];
+    }
+    return 0;
+}
+
+/* The enthalpy RELX_TR takes from an OSZICAR (Read_OSZI, src/util.c:1130-1147). */
+double ref_read_oszi(const char *path) { return Read_OSZI((char *)path); }
+
+/* RDF (src/cell.c:369-417) of one structure as RANK_TR computes it for
+ * duplicate detection: LIST with the cutoff Rmax, then RDF(C, normalise),
+ * with bins NRDF = 3000 over [0, rmax), Gaussian width sigma and taper from
+ * rmin.  out[(pair * 3000 + k)] for the species pairs m <= n in row-major
+ * order.  Returns the bin count. */
+int ref_rdf(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *LAT, double *X, double rmin,
+            double rmax, double sigma, int normalise, double *out) {
+    double *F = (double *)malloc(sizeof(double) * 3 * N), S[6];
+    double *Xc = (double *)malloc(sizeof(double) * 3 * N), rc;
+    int k, m, n, pair;
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    if (!h_ready || strcmp(dir, h_dir) != 0 || N > h_capN || NM != h_capNM)
+        h_call(dir, N, NM, ND, NP, 1, ATMN, LAT, Xc, F, S, 0.0, 0.0);
+    memcpy(Xc, X, sizeof(double) * 3 * N);
+    h_prologue(N, NM, ND, NP, 0.0, 0.0);
+    CAST_CELL(&hC, ATMN, LAT, Xc);
+    rc = hC.Rc;
+    hC.Rc = rmax;
+    hC.Rmax = rmax;
+    hC.Rmin = rmin;
+    hC.DR = sigma;
+    LIST(&hC, 0);
+    RDF(&hC, normalise);
+    hC.Rc = rc;
+    for (m = 0, pair = 0; m < hC.NSPC; m++)
+        for (n = m; n < hC.NSPC; n++, pair++)
+            for (k = 0; k < hC.NRDF; k++) out[(size_t)pair * hC.NRDF + k] = hC.RDF[k][m][n];
+    free(F);
+    free(Xc);
+    return hC.NRDF;
 }

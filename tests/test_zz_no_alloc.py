@@ -1,6 +1,7 @@
 """mb_efs_noalloc: the entry point for callers that own all device memory and
 cannot let the library allocate (see include/maise_b200.h).  It must give the
-same energy, forces and virial as mb_efs for inputs and outputs held in the
+energy, forces and virial of the CPU oracle (the FP64 restatement of the
+reference's CELL_FRC) and of mb_efs, for inputs and outputs held in the
 caller's device buffers, on consecutive calls sharing its fixed scratch
 array.  Collected last so that a run stopping at the first failure has run
 every other test already."""
@@ -11,6 +12,8 @@ import os
 
 import numpy as np
 import pytest
+
+from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -61,10 +64,16 @@ def test_noalloc_matches_mb_efs_on_consecutive_calls(tmp_path):
     small = workloads.fcc_supercell(n=2, a=3.61, jitter=0.05, seed=22)      # 32 atoms, all-pairs path
     cases = [("big", big, _model(tmp_path, big, "big")), ("small", small, _model(tmp_path, small, "small"))]
     pots = {name: maise_b200.Potential(path) for name, _, path in cases}
+    oracle = {name: Oracle(path).efs(w["X"], w["LAT"], w["atmn"], 3, NM=200) for name, w, path in cases}
     # two calls in a row through the shared scratch, then the first structure again
     for name, w, _ in cases + cases[:1]:
         pot = pots[name]
         got = _call_noalloc(pot, w, NM=200)
+        ref = oracle[name]
+        assert got["H"] == pytest.approx(ref["H"], rel=E_RTOL)
+        assert got["E"] == pytest.approx(ref["E"], rel=E_RTOL)
+        np.testing.assert_allclose(got["F"], ref["F"], atol=F_ATOL)
+        np.testing.assert_allclose(got["U"], ref["U"], rtol=E_RTOL, atol=1e-9)
         want = pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=200)
         assert got["H"] == pytest.approx(want["H"], rel=E_RTOL)
         assert got["E"] == pytest.approx(want["E"], rel=E_RTOL)

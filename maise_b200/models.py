@@ -91,7 +91,7 @@ class Basis:
 # model file
 # ---------------------------------------------------------------------------
 
-def write_model(path, spcz, arch, nets, rmin, rmax, basis_text, model_id="B200RAND"):
+def write_model(path, spcz, arch, nets, rmin, rmax, basis_text, model_id="B200RAND", dr=None):
     """Write a model file.
 
     spcz  atomic numbers per species; arch (D, h1, h2)
@@ -119,8 +119,8 @@ def write_model(path, spcz, arch, nets, rmin, rmax, basis_text, model_id="B200RA
     for s in range(nspc):
         for n in range(D):
             lo, hi = float(rmin[s][n]), float(rmax[s][n])
-            dr = 1.0 / (hi - lo) if hi > lo else 1.0
-            out.append(f"  {lo: .16f}   {hi: .16f}   {dr: .16f}")
+            sc = float(dr[s][n]) if dr is not None else (1.0 / (hi - lo) if hi > lo else 1.0)
+            out.append(f"  {lo: .16f}   {hi: .16f}   {sc: .16f}")
     out += [bar, "|                        neural network weights                             |", bar]
     for s in range(nspc):
         w = nets[s]
@@ -131,6 +131,57 @@ def write_model(path, spcz, arch, nets, rmin, rmax, basis_text, model_id="B200RA
     out.append(bar)
     with open(path, "w") as f:
         f.write("\n".join(out) + "\n" + basis_text)
+
+
+def read_model(path):
+    """Parse a model file in the layout write_model emits (the reference's,
+    src/util.c:1233-1335 and src/nutl.c:502-633): dict(spcz, arch (D, h1, h2),
+    nets, rmin, rmax, dr (the input scaling column) [nspc, D], basis_text)."""
+    lines = open(path).read().split("\n")
+
+    def field(key):
+        for ln in lines:
+            if ln.startswith("|") and key in ln:
+                return ln.split("|")[2].strip()
+        raise ValueError(f"{path}: no '{key}'")
+
+    spcz = [int(v) for v in field("species types").split()]
+    D, h1, h2 = (int(v) for v in field("architecture").split()[:3])
+    nspc = len(spcz)
+    k = next(i for i, ln in enumerate(lines) if "input component range" in ln) + 3
+    rng = np.array([[float(v) for v in lines[k + r].split()[:3]] for r in range(nspc * D)]).reshape(nspc, D, 3)
+    k = next(i for i, ln in enumerate(lines) if "neural network weights" in ln) + 2
+    nper = h1 + h2 + 1 + h1 * D + h2 * h1 + h2
+    V = np.array([float(lines[k + r]) for r in range(nspc * nper)])
+    end = k + nspc * nper + 1
+    nets = [nets_from_vector(V[s * nper:(s + 1) * nper], (D, h1, h2)) for s in range(nspc)]
+    return dict(spcz=spcz, arch=(D, h1, h2), nets=nets, rmin=rng[:, :, 0], rmax=rng[:, :, 1], dr=rng[:, :, 2],
+                basis_text="\n".join(lines[end:]))
+
+
+def nets_from_vector(v, arch):
+    """One species' network from its slice of the V2W-ordered parameter
+    vector (src/nmlp.c:591-608): biases b0, b1, b2, then W0, W1, W2."""
+    D, h1, h2 = arch
+    v = np.asarray(v, float)
+    o = 0
+    b0 = v[o:o + h1]; o += h1
+    b1 = v[o:o + h2]; o += h2
+    b2 = float(v[o]); o += 1
+    W0 = v[o:o + h1 * D].reshape(h1, D); o += h1 * D
+    W1 = v[o:o + h2 * h1].reshape(h2, h1); o += h2 * h1
+    W2 = v[o:o + h2].copy()
+    return dict(W0=W0.copy(), b0=b0.copy(), W1=W1.copy(), b1=b1.copy(), W2=W2, b2=b2)
+
+
+def vector_from_nets(nets):
+    """The V2W-ordered parameter vector of all species' networks."""
+    out = []
+    for w in nets:
+        out += list(np.asarray(w["b0"]).reshape(-1)) + list(np.asarray(w["b1"]).reshape(-1)) + [float(w["b2"])]
+        out += list(np.asarray(w["W0"]).reshape(-1)) + list(np.asarray(w["W1"]).reshape(-1))
+        out += list(np.asarray(w["W2"]).reshape(-1))
+    return np.array(out)
 
 
 def random_nets(nspc, arch, seed, binding=None, angular=0.3):

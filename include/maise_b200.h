@@ -87,6 +87,30 @@ int mb_descriptors(mb_potential *pot, int N, int NM, int ND, int XT, const int *
 int mb_descriptor_vjp(mb_potential *pot, int N, int NM, int ND, int XT, const int *atmn, const double *lat9,
                       const double *x, const double *g, double *frc, double *str);
 
+/* Tangent of the descriptor map: dG[N*D] = sum_i (dG/dx_i) . dx_i plus the
+ * response to the homogeneous deformation d -> d + eps d of every neighbour
+ * displacement (eps[9] row-major; either dx or eps may be NULL), with the
+ * derivative parameters of PRS_BP's derivative part (src/nprs.c:567-770).
+ * A unit dx on atom i and axis q is column q of the reference's blocks
+ * Fn[i][.] (dG_j/dx_i for every j); eps = e_a e_b^T is the (a, b) column
+ * of Sn (dG/dstrain, in the virial's convention d_a -> d_a + d_b).  The
+ * adjoint of mb_descriptor_vjp: sum g . dG = -(frc . dx). */
+int mb_descriptor_jvp(mb_potential *pot, int N, int NM, int ND, int XT, const int *atmn, const double *lat9,
+                      const double *x, const double *dx, const double *eps, double *dG);
+
+/* One structure's descriptor file <dir>/e%06d in the layout of LNK_OUT
+ * (src/nprs.c:380-442), as PARS_DAT writes it for training
+ * (src/nprs.c:983-1366): EFS 0 energies only, 1 with derivative blocks of
+ * the marked atoms (marked[N] != 0; their reference forces frc_ref[3N], may
+ * be NULL), 2 with strain blocks of every atom and the reference stresses
+ * str_ref[6] (may be NULL), 3 both.  E, p, DE: the structure's reference
+ * energy, pressure and energy spread for the header; data_path the source
+ * directory recorded in the file.  Neighbour blocks are listed in
+ * ascending atom index. */
+int mb_parse_efile(mb_potential *pot, const char *dir, int index, int EFS, int N, int NM, int ND, int XT,
+                   const int *atmn, const double *lat9, const double *x, double E, double p, double DE,
+                   const int *marked, const double *frc_ref, const double *str_ref, const char *data_path);
+
 /* The neighbour list the E/F/S passes build (LIST, src/cell.c:82-185): for
  * every atom i each (atom j, lattice image) with |x_j + S - x_i|^2 < Rc^2
  * (strict), S = sum_q shift_q L_q, excluding i's own zero image, after the

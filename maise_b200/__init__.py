@@ -56,6 +56,9 @@ def load_library():
     lib.mb_descriptors.argtypes = [vp, c_i, c_i, c_i, c_i, _I, _D, _D, _D]
     lib.mb_descriptor_vjp.argtypes = [vp, c_i, c_i, c_i, c_i, _I, _D, _D, _D, _D, _D]
     lib.mb_neighbours.argtypes = [vp, c_i, c_i, c_i, c_i, _I, _D, _D, c_i, c_i, _I, _I, _I, _D]
+    lib.mb_descriptor_jvp.argtypes = [vp, c_i, c_i, c_i, c_i, _I, _D, _D, _D, _D, _D]
+    lib.mb_parse_efile.argtypes = [vp, ctypes.c_char_p, c_i, c_i, c_i, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_d, _I,
+                                   _D, _D, ctypes.c_char_p]
     lib.mb_relax.argtypes = [vp, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_i, c_i, c_d, _D, _L]
     lib.mb_md_nvt.argtypes = [vp, c_i, c_i, c_i, _I, _D, _D, _D, c_d, c_d, c_d, c_i, c_d, _D, _D, _D]
     lib.mb_maxwell.argtypes = [c_i, _D, c_d, ctypes.c_long, _D]
@@ -270,6 +273,36 @@ class Potential:
                                            cap, nn.ctypes.data_as(_I), nj.ctypes.data_as(_I),
                                            sh.ctypes.data_as(_I), _dp(Xw)))
         return nn, nj.reshape(N, cap), sh.reshape(N, cap, 3), Xw.reshape(N, 3)
+
+    def descriptor_jvp(self, X, LAT, atmn, dx=None, eps=None, ND=3, NM=512, XT=1):
+        """Tangent of the descriptors, [N, D], for atom displacements dx[N, 3]
+        and/or the deformation eps[3, 3] of every neighbour displacement."""
+        atmn = _i32(atmn)
+        N = len(atmn)
+        X = _f64(X, 3 * N)
+        LAT = _f64(LAT, 9)
+        dxa = None if dx is None else _f64(dx, 3 * N)
+        ea = None if eps is None else _f64(eps, 9)
+        dG = np.zeros(N * self.D)
+        self._check(self.lib.mb_descriptor_jvp(self.h, N, NM, ND, XT, atmn.ctypes.data_as(_I), _dp(LAT), _dp(X),
+                                               _dp(dxa), _dp(ea), _dp(dG)))
+        return dG.reshape(N, self.D)
+
+    def parse_efile(self, directory, index, X, LAT, atmn, EFS=1, ND=3, NM=512, XT=1, E=0.0, p=0.0, DE=0.0,
+                    marked=None, frc_ref=None, str_ref=None, data_path="./"):
+        """Write <directory>/e%06d in the reference's parse layout (LNK_OUT)."""
+        atmn = _i32(atmn)
+        N = len(atmn)
+        X = _f64(X, 3 * N)
+        LAT = _f64(LAT, 9)
+        mk = None if marked is None else _i32(np.asarray(marked, bool).astype(np.int32))
+        fr = None if frc_ref is None else _f64(frc_ref, 3 * N)
+        sr = None if str_ref is None else _f64(str_ref, 6)
+        self._check(self.lib.mb_parse_efile(self.h, os.fsencode(directory), index, EFS, N, NM, ND, XT,
+                                            atmn.ctypes.data_as(_I), _dp(LAT), _dp(X), E, p, DE,
+                                            None if mk is None else mk.ctypes.data_as(_I), _dp(fr), _dp(sr),
+                                            os.fsencode(data_path)))
+        return os.path.join(directory, f"e{index:06d}")
 
     def relax(self, X, LAT, atmn, ND=3, NM=512, p_gpa=0.0, urep=0.0, rlxt=3, mitr=100, etol=1e-6):
         """dict(H, X, LAT, n_energy, n_force, iters) -- CELL_RELX/CELL_MIN."""

@@ -23,7 +23,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SOURCES = ["host/mb_model.c", "host/mb_bfgs.c", "host/mb_core.c", "host/mb_call_maise.c", "host/mb_batch.c",
-                "host/mb_surrogate.c", "host/mb_evos.c"]
+                "host/mb_surrogate.c", "host/mb_evos.c", "host/mb_parse.c"]
 CUDA_SOURCES = ["cuda/mb_kernels.cu", "cuda/mb_batch.cu", "cuda/mb_diag.cu", "cuda/mb_static.cu",
                 "cuda/mb_surrogate.cu", "cuda/mb_rdf.cu", "cuda/mb_train.cu"]
 HEADERS = ["mb_internal.h", "host/mb_bfgs.h", "host/mb_batch.h", "host/mb_surrogate_k.h"]

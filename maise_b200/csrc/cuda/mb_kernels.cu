@@ -1839,6 +1839,119 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
 }
 
 /* ------------------------------------------------------------------ */
+/* forward-mode derivative of the descriptors                           */
+/* ------------------------------------------------------------------ */
+
+/* dG = (dG/dx) . dx for a displacement field dx[3N] of the atoms and a
+ * homogeneous deformation eps[3][3] of every neighbour displacement
+ * (d -> d + eps d): the tangent of the descriptor map that the reference
+ * materialises as the derivative blocks Fn (dG_j/dx_i) and Sn (dG/dstrain)
+ * of PRS_BP (src/nprs.c:567-770), with the same species-0 derivative
+ * parameters.  A unit dx on atom m and axis q gives column q of every
+ * Fn block of m; eps = e_a e_b^T gives the (a, b) strain column.
+ * One warp per atom (one per CTA); every term is added to the atom's
+ * descriptor row in shared memory. */
+struct JvpArgs {
+    int N, cap;
+    const int *nn, *nj;
+    const double4 *nd;
+    const int *spc;
+    const mb_params *params;
+    const double *dx;
+    double eps[9];
+    double *dG;
+};
+
+__global__ void __launch_bounds__(32) k_jvp(JvpArgs A) {
+    extern __shared__ __align__(16) char jsm[];
+    const int i = blockIdx.x, lane = threadIdx.x;
+    if (i >= A.N) return;
+    const mb_params &P = *A.params;
+    const int D = P.D, ns = P.nspc, ng2 = P.ng2, cap = A.cap;
+    double4 *d = reinterpret_cast<double4 *>(jsm);
+    double *dd = reinterpret_cast<double *>(d + cap); /* [cap][3] tangent of each displacement */
+    double *g = dd + 3 * cap;                         /* [D] */
+    int *rel = reinterpret_cast<int *>(g + D);        /* [cap] relative species */
+    const int n = A.nn[i], s0 = A.spc[i];
+    for (int t = lane; t < D; t += 32) g[t] = 0.0;
+    for (int t = lane; t < n; t += 32) {
+        const size_t o = (size_t)i * cap + t;
+        const int j = A.nj[o];
+        const double4 v = A.nd[o];
+        d[t] = v;
+        rel[t] = (A.spc[j] - s0 + ns) % ns;
+        const double e[3] = {A.eps[0] * v.x + A.eps[1] * v.y + A.eps[2] * v.z,
+                             A.eps[3] * v.x + A.eps[4] * v.y + A.eps[5] * v.z,
+                             A.eps[6] * v.x + A.eps[7] * v.y + A.eps[8] * v.z};
+        for (int q = 0; q < 3; q++) dd[3 * t + q] = A.dx[3 * j + q] - A.dx[3 * i + q] + e[q];
+    }
+    __syncwarp();
+    /* G2: d/dr [fc(r) exp(-eta (r - rs)^2)] dr, dr = d . dd / r */
+    for (int t = lane; t < n; t += 32) {
+        const double4 v = d[t];
+        const double r = v.w, dr = (v.x * dd[3 * t] + v.y * dd[3 * t + 1] + v.z * dd[3 * t + 2]) / r;
+        double f2, df2;
+        fcut_d(P.d_rc2, r, f2, df2);
+        double *gg = g + P.ind2[rel[t]];
+        for (int f = 0; f < ng2; f++) {
+            const double x = r - P.d_rs[f], eta = P.d_eta2[f];
+            atomicAdd(gg + f, exp(-eta * x * x) * (-2.0 * eta * x * f2 + df2) * dr);
+        }
+    }
+    /* G4 over the pairs a < b of the list (the reference's triplets) */
+    const int ne = P.ne, nzl = P.nzl;
+    for (int a = 0; a + 1 < n; a++) {
+        const double4 d1 = d[a];
+        const double r1 = d1.w;
+        if (!(r1 < P.d_rc4)) continue;
+        const double e1x = dd[3 * a], e1y = dd[3 * a + 1], e1z = dd[3 * a + 2];
+        const double dr1 = (d1.x * e1x + d1.y * e1y + d1.z * e1z) / r1;
+        double f1, df1;
+        fcut_d(P.d_rc4, r1, f1, df1);
+        for (int b = a + 1 + lane; b < n; b += 32) {
+            const double4 d2 = d[b];
+            const double r2 = d2.w;
+            const double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
+            const double r3s = wx * wx + wy * wy + wz * wz;
+            if (!(r2 < P.d_rc4 && r3s < P.d_rc4sq)) continue;
+            const double r3 = sqrt(r3s);
+            const double e2x = dd[3 * b], e2y = dd[3 * b + 1], e2z = dd[3 * b + 2];
+            const double dr2 = (d2.x * e2x + d2.y * e2y + d2.z * e2z) / r2;
+            const double dr3 = (wx * (e2x - e1x) + wy * (e2y - e1y) + wz * (e2z - e1z)) / r3;
+            const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) / (r1 * r2);
+            const double dc = (e1x * d2.x + e1y * d2.y + e1z * d2.z + d1.x * e2x + d1.y * e2y + d1.z * e2z) / (r1 * r2) -
+                              c * (dr1 / r1 + dr2 / r2);
+            double f2, df2, f3, df3;
+            fcut_d(P.d_rc4, r2, f2, df2);
+            fcut_d(P.d_rc4, r3, f3, df3);
+            const double Af = 2.0 * f1 * f2 * f3;
+            const double dA = 2.0 * (df1 * dr1 * f2 * f3 + f1 * df2 * dr2 * f3 + f1 * f2 * df3 * dr3);
+            const double rr = r1 * r1 + r2 * r2 + r3s, drr = r1 * dr1 + r2 * dr2 + r3 * dr3;
+            double sv[MB_MAXE], tv[MB_MAXE];
+            for (int e = 0; e < ne; e++) {
+                const double eta = P.d_eta4[e], E = exp(-eta * rr);
+                sv[e] = dA * E + Af * E * (-2.0 * eta * drr);
+                tv[e] = Af * E * dc;
+            }
+            double lz[MB_MAXZL], lzp[MB_MAXZL];
+            for (int k = 0; k < MB_MAXZL; k++) lz[k] = lzp[k] = 0.0;
+            angular<8, 4>(P, c, lz, lzp);
+            /* angular<8, 4> lays (zeta, lambda) out as z * 4 + l */
+            const int va = rel[a], vb = rel[b];
+            const int lo = va < vb ? va : vb, hi = va < vb ? vb : va;
+            double *gg = g + P.ind4[lo * lo + hi * hi];
+            for (int f = 0; f < P.ng4; f++) {
+                const int e = P.g4_e[f], zl = (P.g4_zl[f] / P.nlam) * 4 + P.g4_zl[f] % P.nlam;
+                atomicAdd(gg + f, sv[e] * lz[zl] + tv[e] * lzp[zl]);
+            }
+        }
+    }
+    (void)nzl;
+    __syncwarp();
+    for (int t = lane; t < D; t += 32) A.dG[(size_t)i * D + t] = g[t];
+}
+
+/* ------------------------------------------------------------------ */
 /* reductions                                                          */
 /* ------------------------------------------------------------------ */
 
@@ -2285,6 +2398,34 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
     int rc = launch_any(m, shape, a, st, e0, e1);
     (*launches)++;
     return rc;
+}
+
+/* the descriptor tangent for displacements dx[3N] (device) and the
+ * deformation eps[9] (host), into dG[N*D] (device) */
+extern "C" int mbk_jvp(mb_dev *d, const mb_model *m, int N, const double *dx, const double *eps, double *dG,
+                       void *stream, long *launches) {
+    if (m->P.nz > 8 || m->P.nlam > 4) return (int)cudaErrorInvalidValue;
+    JvpArgs a;
+    a.N = N;
+    a.cap = d->capNB;
+    a.nn = d->nn;
+    a.nj = d->nj;
+    a.nd = (const double4 *)d->nd;
+    a.spc = d->spc;
+    a.params = d->params;
+    a.dx = dx;
+    for (int k = 0; k < 9; k++) a.eps[k] = eps ? eps[k] : 0.0;
+    a.dG = dG;
+    const size_t smem = sizeof(double4) * d->capNB + sizeof(double) * (3 * (size_t)d->capNB + m->P.D) +
+                        sizeof(int) * d->capNB;
+    if (smem > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_jvp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    k_jvp<<<N, 32, smem, (cudaStream_t)stream>>>(a);
+    (*launches)++;
+    return (int)cudaGetLastError();
 }
 
 extern "C" int mbk_finalize(mb_dev *d, int N, int mode, double pV, void *stream, long *launches) {

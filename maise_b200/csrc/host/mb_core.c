@@ -821,6 +821,44 @@ out:
     return r;
 }
 
+int mb_descriptor_jvp(mb_potential *p, int N, int NM, int ND, int XT, const int *atmn, const double *lat9,
+                      const double *x, const double *dx, const double *eps, double *dG) {
+    mb_cell c;
+    int r, tries, ncell;
+    if (!p || N < 1 || NM < 1 || ND < 0 || ND > 3 || !atmn || !lat9 || !x || !dG || (!dx && !eps))
+        return fail(MB_ERR_ARG, "bad arguments");
+    CK(cudaSetDevice(p->device), "cudaSetDevice");
+    setup_cell(p, lat9, ND, N, &c);
+    ncell = c.M[0] ? c.M[0] * c.M[1] * c.M[2] : 1;
+    if ((r = ensure(p, N, p->d.capNB ? p->d.capNB : (NM < 64 ? NM : 64), ncell))) return r;
+    p->d.legs_on = 0;
+    for (tries = 0; tries < 3; tries++) {
+        if ((r = upload(p, N, XT, atmn, lat9, x))) return r;
+        CK(cudaMemsetAsync(p->d.status, 0, sizeof(int) * 4, p->stream), "memset status");
+        if ((r = mbk_wrap(&p->d, N, &c, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "wrap");
+        if ((r = mbk_nlist(&p->d, N, NM, &c, p->m.rc_list, p->stream, &p->launches)))
+            return cuda_fail((cudaError_t)r, "neighbour list");
+        CK(cudaMemcpyAsync(p->h_status, p->d.status, sizeof(int) * 4, cudaMemcpyDeviceToHost, p->stream), "D2H status");
+        CK(cudaStreamSynchronize(p->stream), "synchronize");
+        if (p->h_status[0] & MB_ST_WRAP) return fail(MB_ERR_STATE, "non-finite or runaway positions");
+        if (p->h_status[0] & MB_ST_NBR_OVERFLOW)
+            return fail(MB_ERR_NEIGHBOURS, "an atom reached NM=%d neighbours within %.4f A; increase NM", NM, p->m.rc_list);
+        if (!(p->h_status[0] & MB_ST_CAP_OVERFLOW)) break;
+        if ((r = ensure(p, N, p->h_status[1] + 8, ncell))) return r;
+    }
+    if (tries == 3) return fail(MB_ERR_CAPACITY, "neighbour capacity could not be established");
+    /* the displacement tangent goes to the force buffer, which no pass keeps */
+    if (dx)
+        CK(cudaMemcpyAsync(p->d.F, dx, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, p->stream), "H2D dx");
+    else
+        CK(cudaMemsetAsync(p->d.F, 0, sizeof(double) * 3 * N, p->stream), "memset dx");
+    if ((r = mbk_jvp(&p->d, &p->m, N, p->d.F, eps, p->d.G, p->stream, &p->launches)))
+        return cuda_fail((cudaError_t)r, "descriptor tangent kernel");
+    CK(cudaMemcpyAsync(dG, p->d.G, sizeof(double) * (size_t)N * p->m.P.D, cudaMemcpyDeviceToHost, p->stream), "D2H dG");
+    CK(cudaStreamSynchronize(p->stream), "synchronize");
+    return MB_OK;
+}
+
 /* ------------------------------------------------------------------ */
 /* relaxation (CELL_MIN, src/cmin.c)                                   */
 /* ------------------------------------------------------------------ */

@@ -155,6 +155,8 @@ int mbk_nlist(mb_dev *d, int N, int NM, const mb_cell *c, double rc, void *strea
 int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode, double urep, int need_nb_max, int nb_max,
                         void *stream, long *launches);
 int mbk_finalize(mb_dev *d, int N, int mode, double pV, void *stream, long *launches);
+int mbk_jvp(mb_dev *d, const mb_model *m, int N, const double *dx, const double *eps, double *dG, void *stream,
+            long *launches);
 int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, void *stream,
                    long *launches);
 int mbk_set_out(mb_dev *d, int idx, double v, void *stream);

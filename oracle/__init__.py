@@ -209,6 +209,9 @@ class RefOracle:
             lib.ref_read_cell.argtypes = [ctypes.c_char_p, c_i, _I, _D, _D, _I]
             lib.ref_read_oszi.restype = c_d
             lib.ref_rdf.argtypes = [ctypes.c_char_p, c_i, c_i, c_i, c_i, _I, _D, _D, c_d, c_d, c_d, c_i, _D]
+            lib.ref_efile_read.argtypes = [ctypes.c_char_p, c_i, _I, _D, _I, _D]
+            lib.ref_efile_block.argtypes = [c_i, _I, _I, _D, _D]
+            lib.ref_efile_sn.argtypes = [_D, _D]
             lib.ref_read_oszi.argtypes = [ctypes.c_char_p]
             cls._lib = lib
         return cls._lib
@@ -305,6 +308,36 @@ class RefOracle:
         nb = self.lib().ref_rdf(self.dir, len(atmn), NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), rmin, rmax,
                                 sigma, int(normalise), _dp(out))
         return out.reshape(npair, nb)
+
+    @classmethod
+    def read_efile(cls, directory, index, maxN=4096, maxD=1024):
+        """A descriptor file read by the reference's LNK_IN: dict(EFS, D, N, NF,
+        E, p, DE, atmn, Cn, blocks {atom: (dni, F, Fn[dnn+1, D, 3])}, S, Sn)."""
+        lib = cls.lib()
+        hdr = np.zeros(4, np.int32)
+        eh = np.zeros(3)
+        atmn = np.zeros(maxN, np.int32)
+        Cn = np.zeros(maxN * maxD)
+        if lib.ref_efile_read(os.fsencode(directory), index, _ip(hdr), _dp(eh), _ip(atmn), _dp(Cn)):
+            raise RuntimeError("LNK_IN failed")
+        EFS, D, N, NF = (int(v) for v in hdr)
+        out = dict(EFS=EFS, D=D, N=N, NF=NF, E=eh[0], p=eh[1], DE=eh[2], atmn=atmn[:N].copy(),
+                   Cn=Cn[:N * D].reshape(N, D).copy(), blocks={})
+        if EFS in (1, 3):
+            for i in range(N):
+                dnn = ctypes.c_int()
+                dni = np.zeros(1024, np.int32)
+                F = np.zeros(3)
+                fn = np.zeros(1025 * D * 3)
+                if lib.ref_efile_block(i, ctypes.byref(dnn), _ip(dni), _dp(F), _dp(fn)) == 0:
+                    k = dnn.value
+                    out["blocks"][i] = (dni[:k].copy(), F, fn[:(k + 1) * D * 3].reshape(k + 1, D, 3))
+        if EFS in (2, 3):
+            sn = np.zeros(N * D * 6)
+            S = np.zeros(6)
+            lib.ref_efile_sn(_dp(sn), _dp(S))
+            out["S"], out["Sn"] = S, sn.reshape(N, D, 6)
+        return out
 
     def read_oszi(self, path):
         """The enthalpy Read_OSZI takes from an OSZICAR."""

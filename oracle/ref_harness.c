@@ -384,3 +384,62 @@ int ref_rdf(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *L
     free(Xc);
     return hC.NRDF;
 }
+
+/* A descriptor file read back by the reference's LNK_IN (src/nprs.c:308-377)
+ * into a private LNK: hdr = {EFS, D, N, NF}, ehdr = {E, p, DE}, atmn[N],
+ * Cn[N*D]; then ref_efile_block reads one marked atom's blocks and
+ * ref_efile_sn the strain blocks. */
+static LNK eL;
+static int eEFS, eD;
+int ref_efile_read(const char *dir, int o, int *hdr, double *ehdr, int *atmn, double *Cn) {
+    char buf[1200];
+    FILE *in;
+    int i, n, N, NF, DNn;
+    snprintf(buf, sizeof(buf), "%s/e%06d", dir, o);
+    if (!(in = fopen(buf, "r"))) return -1;
+    if (fscanf(in, "%d %d %d %d %d", &eEFS, &eD, &N, &NF, &DNn) != 5) {
+        fclose(in);
+        return -1;
+    }
+    fclose(in);
+    memset(&eL, 0, sizeof(eL));
+    LNK_IN(&eL, o, (char *)dir);
+    hdr[0] = eEFS;
+    hdr[1] = eD;
+    hdr[2] = eL.N;
+    hdr[3] = eL.NF;
+    ehdr[0] = eL.E;
+    ehdr[1] = eL.p;
+    ehdr[2] = eL.DE;
+    for (i = 0; i < eL.N; i++) {
+        atmn[i] = eL.ATMN[i];
+        for (n = 0; n < eD; n++) Cn[(size_t)i * eD + n] = eL.Cn[i][n];
+    }
+    return 0;
+}
+
+/* Blocks of marked atom i from the last ref_efile_read: dnn, dni[dnn], the
+ * reference force F[3] and fn[(slot*D+n)*3+q] with slot dnn the self block. */
+int ref_efile_block(int i, int *dnn, int *dni, double *F, double *fn) {
+    int j, n, q;
+    if (!(eEFS == 1 || eEFS == 3) || !eL.MRK[i]) return -1;
+    *dnn = eL.DNn[i];
+    for (q = 0; q < 3; q++) F[q] = eL.F[i][q];
+    for (j = 0; j <= *dnn; j++) {
+        if (j < *dnn) dni[j] = eL.DNi[i][j];
+        for (n = 0; n < eD; n++)
+            for (q = 0; q < 3; q++) fn[((size_t)j * eD + n) * 3 + q] = eL.Fn[i][j][n][q];
+    }
+    return 0;
+}
+
+/* Strain blocks sn[(i*D+n)*6+k] and the reference stresses S[6]. */
+int ref_efile_sn(double *sn, double *S) {
+    int i, n, k;
+    if (!(eEFS == 2 || eEFS == 3)) return -1;
+    for (k = 0; k < 6; k++) S[k] = eL.S[k];
+    for (i = 0; i < eL.N; i++)
+        for (n = 0; n < eD; n++)
+            for (k = 0; k < 6; k++) sn[((size_t)i * eD + n) * 6 + k] = eL.Sn[i][n][k];
+    return 0;
+}

@@ -106,7 +106,9 @@ int mb_descriptor_jvp(mb_potential *pot, int N, int NM, int ND, int XT, const in
  * str_ref[6] (may be NULL), 3 both.  E, p, DE: the structure's reference
  * energy, pressure and energy spread for the header; data_path the source
  * directory recorded in the file.  Neighbour blocks are listed in
- * ascending atom index. */
+ * ascending atom index; an atom that is its own periodic neighbour has its
+ * whole dG_i/dx_i in the self block (the reference splits off the part
+ * through i's images into a block listed under i). */
 int mb_parse_efile(mb_potential *pot, const char *dir, int index, int EFS, int N, int NM, int ND, int XT,
                    const int *atmn, const double *lat9, const double *x, double E, double p, double DE,
                    const int *marked, const double *frc_ref, const double *str_ref, const char *data_path);

@@ -888,9 +888,10 @@ __global__ void __launch_bounds__(WPA * 32 * APB, APB >= 4 ? 2 : 1) k_efs(EfsArg
                     tl_whole &= for_block<WPA, RUN_CONVERGED>(s, a, b, blk, 0, tl_pos, tl_lo, tl_hi, warp, lane, accept_blk, body);
                     group_sync<WPA>();
                     group_store64<WPA>(c0, c1, s, warp, lane);
-                    if (tid == 0) {
+                    {
+                        /* every feature is its own descriptor entry: one per thread */
                         const int base = P.ind4[a * a + b * b];
-                        for (int f = 0; f < P.ng4; f++)
+                        for (int f = tid; f < P.ng4; f += NT)
                             s.G[base + f] += s.red[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam];
                     }
                     group_sync<WPA>();
@@ -932,9 +933,9 @@ __global__ void __launch_bounds__(WPA * 32 * APB, APB >= 4 ? 2 : 1) k_efs(EfsArg
 #pragma unroll
                 for (int ch = 0; ch < CELLS / 64; ch++) {
                     group_reduce64<WPA>(acc + 64 * ch, s, warp, lane);
-                    if (tid == 0) {
+                    {
                         int ds = a * a + b * b, base = P.ind4[ds];
-                        for (int f = 0; f < P.ng4; f++) {
+                        for (int f = tid; f < P.ng4; f += NT) {
                             int cell = P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam;
                             if (cell / 64 == ch) s.G[base + f] += s.red[cell % 64];
                         }
@@ -1051,9 +1052,8 @@ __global__ void __launch_bounds__(WPA * 32 * APB, APB >= 4 ? 2 : 1) k_efs(EfsArg
                 const int ds = a * a + b * b, base = P.ind4[ds];
                 for (int t = tid; t < NE * NZL; t += NT) s.grid[t] = 0.0;
                 group_sync<WPA>();
-                if (tid == 0)
-                    for (int f = 0; f < P.ng4; f++)
-                        s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam] += s.G[base + f];
+                for (int f = tid; f < P.ng4; f += NT)
+                    atomicAdd(&s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam], s.G[base + f]);
                 group_sync<WPA>();
                 /* returns the entry's force on neighbour j; run_list_runs sums
                  * those per lane and adds them once per change of j */
@@ -1474,9 +1474,10 @@ __device__ __forceinline__ int leg_block(const LegSmem &s, const unsigned *__res
  * (i-j and i-k from i's own rows, staged; j-k from j's row in global
  * memory, L2-resident).  Reference bases: at most 8 G4 exponents, zeta in
  * {1, 2, 4, 16} or other integers, 2 lambdas. */
-template <int WPA, int APB>
+template <int NE, int WPA, int APB>
 __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
-    constexpr int NZ = 4, NLAM = 2, NZL = 8, NE = 8;
+    constexpr int NZ = 4, NLAM = 2, NZL = 8;
+    static_assert(NE == 7 || NE == 8, "leg rows hold 8 exponents");
     extern __shared__ __align__(16) char smem_raw[];
     __shared__ mb_params Ps;
     {
@@ -1606,10 +1607,10 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
                         const double A3 = 2.0 * la[4].x * lb[4].x * __ldg(lg + 4).x;
                         angular<NZ, NLAM>(P, c, lz, nullptr);
 #pragma unroll
-                        for (int hh = 0; hh < NE / 2; hh++) {
+                        for (int hh = 0; hh < (NE + 1) / 2; hh++) {
                             const double2 x = la[hh], y = lb[hh], z = __ldg(lg + hh);
                             ex[2 * hh] = A3 * (x.x * y.x) * z.x;
-                            ex[2 * hh + 1] = A3 * (x.y * y.y) * z.y;
+                            if (2 * hh + 1 < NE) ex[2 * hh + 1] = A3 * (x.y * y.y) * z.y;
                         }
                     }
                     double *rw = stw + lane * EFS_STG;
@@ -1632,9 +1633,9 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
                                                           tl_hi, warp, lane, body);
                 group_sync<WPA>();
                 group_store64<WPA>(c0, c1, s, warp, lane);
-                if (tid == 0) {
+                {
                     const int base = P.ind4[al * al + be * be];
-                    for (int f = 0; f < P.ng4; f++)
+                    for (int f = tid; f < P.ng4; f += NT)
                         s.G[base + f] += s.red[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam];
                 }
                 group_sync<WPA>();
@@ -1741,9 +1742,8 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
                 const int base = P.ind4[al * al + be * be];
                 for (int t = tid; t < 64; t += NT) s.grid[t] = 0.0;
                 group_sync<WPA>();
-                if (tid == 0)
-                    for (int f = 0; f < P.ng4; f++)
-                        s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam] += s.G[base + f];
+                for (int f = tid; f < P.ng4; f += NT)
+                    atomicAdd(&s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam], s.G[base + f]);
                 group_sync<WPA>();
                 auto body = [&](unsigned ent) -> double3 {
                     const int a = (int)(ent & 0xffu), b = (int)((ent >> 8) & 0xffu), cj = (int)(ent >> 16);
@@ -1762,11 +1762,12 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
                     angular<NZ, NLAM>(P, c, lz, lzp);
                     double Q = 0.0, Qe = 0.0, Qc = 0.0;
 #pragma unroll
-                    for (int hh = 0; hh < NE / 2; hh++) {
+                    for (int hh = 0; hh < (NE + 1) / 2; hh++) {
                         const double2 x = la[hh], y = lb[hh], z = __ldg(lg + hh);
 #pragma unroll
                         for (int q = 0; q < 2; q++) {
                             const int e = 2 * hh + q;
+                            if (e >= NE) break;
                             const double E = q ? (x.y * y.y) * z.y : (x.x * y.x) * z.x;
                             double u = 0.0, v = 0.0;
 #pragma unroll
@@ -1816,18 +1817,26 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
         vr[3] += fx * d.y; vr[4] += fy * d.z; vr[5] += fz * d.x;
     }
     {
-        double v[64];
+        /* the atom's force and virial: warp sums, then the warps in a fixed order */
+        double v[9] = {fi[0], fi[1], fi[2], vr[0], vr[1], vr[2], vr[3], vr[4], vr[5]};
 #pragma unroll
-        for (int k = 0; k < 64; k++) v[k] = 0.0;
-        v[0] = fi[0]; v[1] = fi[1]; v[2] = fi[2];
-#pragma unroll
-        for (int k = 0; k < 6; k++) v[3 + k] = vr[k];
-        group_reduce64<WPA>(v, s, warp, lane);
+        for (int k = 0; k < 9; k++) v[k] = warp_sum(v[k]);
+        if (WPA > 1) {
+            if (lane == 0)
+                for (int k = 0; k < 9; k++) s.red[warp * 9 + k] = v[k];
+            group_sync<WPA>();
+            if (tid == 0)
+                for (int k = 0; k < 9; k++) {
+                    double t = 0.0;
+                    for (int w = 0; w < WPA; w++) t += s.red[w * 9 + k];
+                    v[k] = t;
+                }
+        }
         if (tid == 0) {
-            atomicAdd(&A.F[3 * i], s.red[0]);
-            atomicAdd(&A.F[3 * i + 1], s.red[1]);
-            atomicAdd(&A.F[3 * i + 2], s.red[2]);
-            for (int k = 0; k < 6; k++) A.vir[(size_t)i * 6 + k] = s.red[3 + k];
+            atomicAdd(&A.F[3 * i], v[0]);
+            atomicAdd(&A.F[3 * i + 1], v[1]);
+            atomicAdd(&A.F[3 * i + 2], v[2]);
+            for (int k = 0; k < 6; k++) A.vir[(size_t)i * 6 + k] = v[3 + k];
         }
         for (int t = tid; t < n; t += NT) {
             const int j = s.j[t];
@@ -2207,9 +2216,9 @@ static size_t leg_group_bytes(const mb_model *m, int capNB, int wpa) {
     return leg_smem_bytes(capNB, m->P.D, m->P.ng2, wpa, tl_entries_leg(capNB, wpa));
 }
 
-template <int WPA, int APB>
+template <int NE, int WPA, int APB>
 static int launch_leg(const LegArgs &a, cudaStream_t st) {
-    auto kern = k_efs_leg<WPA, APB>;
+    auto kern = k_efs_leg<NE, WPA, APB>;
     const size_t smem = a.smem_group * APB;
     static size_t configured[MB_MAX_DEVICES_K] = {0};
     int dev = 0;
@@ -2233,11 +2242,20 @@ static int launch_leg_pass(const mb_dev *d, const mb_model *m, int shape, LegArg
     k_legs<<<(a.N + 3) / 4, 128, 0, st>>>(a.N, a.cap, d->nn, d->nj, d->nk, (double4 *)d->nd, d->spc, d->params,
                                          d->leg, d->nso);
     int rc;
-    switch (shape) {
-        case 0: rc = launch_leg<1, 4>(a, st); break;
-        case 1: rc = launch_leg<1, 2>(a, st); break;
-        case 2: rc = launch_leg<2, 1>(a, st); break;
-        default: rc = launch_leg<4, 1>(a, st); break;
+    if (m->P.ne <= 7) {
+        switch (shape) {
+            case 0: rc = launch_leg<7, 1, 4>(a, st); break;
+            case 1: rc = launch_leg<7, 1, 2>(a, st); break;
+            case 2: rc = launch_leg<7, 2, 1>(a, st); break;
+            default: rc = launch_leg<7, 4, 1>(a, st); break;
+        }
+    } else {
+        switch (shape) {
+            case 0: rc = launch_leg<8, 1, 4>(a, st); break;
+            case 1: rc = launch_leg<8, 1, 2>(a, st); break;
+            case 2: rc = launch_leg<8, 2, 1>(a, st); break;
+            default: rc = launch_leg<8, 4, 1>(a, st); break;
+        }
     }
     if (e1) mbk_record(e1, st);
     return rc;

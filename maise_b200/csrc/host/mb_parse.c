@@ -18,7 +18,11 @@
  * along axis q gives column q of all of i's blocks at once; a unit
  * deformation gives one strain column of every atom.  The neighbour atoms
  * of a marked atom are listed in ascending index (the reference lists them
- * in its neighbour-list order; the blocks are the same).
+ * in its neighbour-list order).  An atom that is its own periodic neighbour
+ * has one self block holding the whole dG_i/dx_i; the reference keeps the
+ * part that comes through i's images in a second block listed under i's
+ * own index.  The contraction the force training makes of the blocks
+ * (FRC_ANN, src/nmlp.c:433-479) is the same either way.
  */
 #include <stdio.h>
 #include <stdlib.h>

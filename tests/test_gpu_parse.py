@@ -41,6 +41,17 @@ def test_tangent_is_the_adjoint_of_the_vjp(mb, tmp_path):
     assert lhs == pytest.approx(rhs, rel=1e-10, abs=1e-10)
 
 
+def golden_total(dni, Fn, atom, owner):
+    """dG_owner/dx_atom from the reference's blocks: the reference keeps the
+    part of an atom's own descriptors that comes through its periodic images
+    in a separate block listed under its own index, beside the self block
+    (slot dnn); the tangent gives their sum."""
+    tot = sum(Fn[slot] for slot, o in enumerate(dni) if o == owner)
+    if owner == atom:
+        tot = tot + Fn[len(dni)]
+    return tot
+
+
 def test_tangent_gives_the_golden_derivative_blocks(mb, parse_golden, parse_model_dir):
     pot = mb.Potential(parse_model_dir + "/model")
     off = parse_golden["offsets"]
@@ -55,9 +66,8 @@ def test_tangent_gives_the_golden_derivative_blocks(mb, parse_golden, parse_mode
             cols.append(pot.descriptor_jvp(X, L, at, dx=dx, ND=3, NM=400))
         blk = np.stack(cols, axis=-1)  # [owner, n, q]
         dni, Fn = parse_golden["mk_dni"][k], parse_golden["mk_fn"][k]
-        np.testing.assert_allclose(blk[atom], Fn[len(dni)], atol=1e-10)
-        for slot, o in enumerate(dni):
-            np.testing.assert_allclose(blk[o], Fn[slot], atol=1e-10)
+        for o in set(dni.tolist()) | {atom}:
+            np.testing.assert_allclose(blk[o], golden_total(dni, Fn, atom, o), atol=1e-10)
         # no atom outside the reference's list depends on this atom
         others = np.setdiff1d(np.arange(len(at)), np.concatenate([dni, [atom]]))
         assert np.abs(blk[others]).max(initial=0.0) == 0.0
@@ -99,7 +109,9 @@ def test_descriptor_files_read_back_by_lnk_in(mb, parse_golden, parse_model_dir,
                         marked=marked, frc_ref=F, str_ref=np.arange(6.0), data_path=f"./DATA/{s}/")
         r = RefOracle.read_efile(str(tmp_path), idx)
         assert (r["EFS"], r["D"], r["N"], r["NF"]) == (EFS, 82, N, int(marked.sum()))
-        assert (r["E"], r["p"], r["DE"]) == pytest.approx((-2.5 * N, 1.25, 0.5), abs=1e-6)
+        assert (r["E"], r["DE"]) == pytest.approx((-2.5 * N, 0.5), abs=1e-6)
+        head = open(tmp_path / f"e{idx:06d}").readline().split()
+        assert float(head[6]) == pytest.approx(1.25)  # LNK_IN reads the pressure but Build_LNK resets it
         np.testing.assert_array_equal(r["atmn"], at)
         np.testing.assert_allclose(r["Cn"], parse_golden["G"][a:b], rtol=1e-12, atol=1e-13)
         for k in marked_by_struct.get(s, []):
@@ -107,10 +119,10 @@ def test_descriptor_files_read_back_by_lnk_in(mb, parse_golden, parse_model_dir,
             dni, Fr, Fn = r["blocks"][atom]
             np.testing.assert_allclose(Fr, F[atom], atol=1e-6)
             gdni, gFn = parse_golden["mk_dni"][k], parse_golden["mk_fn"][k]
-            assert sorted(dni) == sorted(gdni)
-            np.testing.assert_allclose(Fn[len(dni)], gFn[len(gdni)], atol=1e-10)
-            for slot, o in enumerate(gdni):
-                np.testing.assert_allclose(Fn[list(dni).index(o)], gFn[slot], atol=1e-10)
+            assert sorted(dni) == sorted(set(gdni.tolist()) - {atom})
+            np.testing.assert_allclose(Fn[len(dni)], golden_total(gdni, gFn, atom, atom), atol=1e-10)
+            for slot, o in enumerate(dni):
+                np.testing.assert_allclose(Fn[slot], golden_total(gdni, gFn, atom, o), atol=1e-10)
         if EFS == 3:
             np.testing.assert_allclose(r["S"], np.arange(6.0))
             assert r["Sn"].shape == (N, 82, 6)

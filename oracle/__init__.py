@@ -212,6 +212,8 @@ class RefOracle:
             lib.ref_efile_read.argtypes = [ctypes.c_char_p, c_i, _I, _D, _I, _D]
             lib.ref_efile_block.argtypes = [c_i, _I, _I, _D, _D]
             lib.ref_efile_sn.argtypes = [_D, _D]
+            lib.ref_train_terms.restype = c_d
+            lib.ref_train_terms.argtypes = [c_i, c_i, c_i, c_i, _D, _D, _D, c_d, c_d, c_d, _D, _D, _D]
             lib.ref_read_oszi.argtypes = [ctypes.c_char_p]
             cls._lib = lib
         return cls._lib
@@ -338,6 +340,29 @@ class RefOracle:
             lib.ref_efile_sn(_dp(sn), _dp(S))
             out["S"], out["Sn"] = S, sn.reshape(N, D, 6)
         return out
+
+    @classmethod
+    def train_terms(cls, directory, index, V, nspc, D, h1, h2, rmin, dr, WE=1.0, WF=1.0, w=1.0):
+        """The training terms of descriptor file `index` through the reference's
+        LNK_IN, ADJT_LNK, FRC_ANN_PARA, DE_ANN_PARA and DF_ANN_PARA:
+        (E, f[N, 3] on the marked atoms, gE, gF) with the gradient terms in
+        dfunc_gsl's order, not yet divided by the number of structures."""
+        lib = cls.lib()
+        hdr = np.zeros(4, np.int32)
+        eh = np.zeros(3)
+        atmn = np.zeros(4096, np.int32)
+        Cn = np.zeros(4096 * 1024)
+        if lib.ref_efile_read(os.fsencode(directory), index, _ip(hdr), _dp(eh), _ip(atmn), _dp(Cn)):
+            raise RuntimeError("LNK_IN failed")
+        N = int(hdr[2])
+        V = np.ascontiguousarray(V, float)
+        rmin = np.ascontiguousarray(rmin, float).reshape(-1)
+        dr = np.ascontiguousarray(dr, float).reshape(-1)
+        f = np.zeros(3 * N)
+        gE = np.zeros(len(V))
+        gF = np.zeros(len(V))
+        E = lib.ref_train_terms(nspc, D, h1, h2, _dp(V), _dp(rmin), _dp(dr), WE, WF, w, _dp(f), _dp(gE), _dp(gF))
+        return float(E), f.reshape(N, 3), gE, gF
 
     def read_oszi(self, path):
         """The enthalpy Read_OSZI takes from an OSZICAR."""

@@ -390,7 +390,7 @@ int ref_rdf(const char *dir, int N, int NM, int ND, int NP, int *ATMN, double *L
  * Cn[N*D]; then ref_efile_block reads one marked atom's blocks and
  * ref_efile_sn the strain blocks. */
 static LNK eL;
-static int eEFS, eD;
+static int eEFS, eD, eScaled;
 int ref_efile_read(const char *dir, int o, int *hdr, double *ehdr, int *atmn, double *Cn) {
     char buf[1200];
     FILE *in;
@@ -404,6 +404,7 @@ int ref_efile_read(const char *dir, int o, int *hdr, double *ehdr, int *atmn, do
     fclose(in);
     memset(&eL, 0, sizeof(eL));
     LNK_IN(&eL, o, (char *)dir);
+    eScaled = 0;
     hdr[0] = eEFS;
     hdr[1] = eD;
     hdr[2] = eL.N;
@@ -442,4 +443,104 @@ int ref_efile_sn(double *sn, double *S) {
         for (n = 0; n < eD; n++)
             for (k = 0; k < 6; k++) sn[((size_t)i * eD + n) * 6 + k] = eL.Sn[i][n][k];
     return 0;
+}
+
+/* The training terms of the last ref_efile_read structure through the
+ * reference's own functions: the network V (V2W order, src/nmlp.c:591-608;
+ * nspc species, D-h1-h2-1, tanh hidden layers) with input table rmin/dr
+ * [nspc*D]; ADJT_LNK (src/nmod.c:244-259) puts Cn (and, for EFS 1, Fn) on
+ * the input scale -- once per read; then
+ *   E = FRC_ANN_PARA (src/nmlp.c:29-102), f[3N] the forces it leaves on
+ *       the marked atoms (0 elsewhere),
+ *   gE = DE_ANN_PARA's accumulation (src/nmlp.c:292-354) and
+ *   gF = DF_ANN_PARA's (src/nmlp.c:104-290), each in dfunc_gsl's order
+ *       (src/nmin.c:280-295: per species biases, then weights), not yet
+ *       divided by the number of structures.
+ * w is the structure's weight L->W. */
+double ref_train_terms(int nspc, int D, int h1, int h2, const double *V, const double *rmin, const double *dr,
+                       double WE, double WF, double w, double *f, double *gE, double *gF) {
+    ANN R;
+    int s, k, m, n, i, mx, dnm = 0;
+    double E, ***e, ***d, ***c, ***xn, ***xm, ***Bp, ****Wp;
+    if (eD != D) return NAN;
+    memset(&R, 0, sizeof(R));
+    R.NSPC = nspc;
+    R.D = D;
+    R.NL = 4;
+    R.NU[0] = D; R.NU[1] = h1; R.NU[2] = h2; R.NU[3] = 1;
+    R.GT[0] = 0; R.GT[1] = 1; R.GT[2] = 1; R.GT[3] = 0;
+    R.MIX = 0;
+    R.O = 0;
+    R.STR = 1;
+    R.EFS = eEFS;
+    R.WE = WE;
+    R.WF = WF;
+    mx = D > h1 ? D : h1;
+    if (h2 > mx) mx = h2;
+    R.B = make_d3D(nspc, 3, mx);
+    R.W = make_d4D(nspc, 3, mx, mx);
+    R.Rmin = make_d2D(nspc, D);
+    R.DR = make_d2D(nspc, D);
+    for (s = 0; s < nspc; s++)
+        for (n = 0; n < D; n++) {
+            R.Rmin[s][n] = rmin[s * D + n];
+            R.DR[s][n] = dr[s * D + n];
+        }
+    V2W(&R, (double *)V);
+    if (!eScaled) {
+        /* Build_LNK leaves DNs unset for unmarked atoms (src/nutl.c:379-387)
+         * and ADJT_LNK indexes DR with DNs[i][0] of every atom
+         * (src/nmod.c:254-257): give those unused rows a valid species */
+        if (eEFS == 1 || eEFS == 3)
+            for (i = 0; i < eL.N; i++)
+                if (!eL.MRK[i]) eL.DNs[i][0] = eL.ATMN[i];
+        ADJT_LNK(&R, &eL);
+        eScaled = 1;
+    }
+    eL.W = w;
+    for (i = 0; i < eL.N; i++)
+        if (eL.DNn[i] > dnm) dnm = eL.DNn[i];
+    e = make_d3D(eL.N, 4, mx);
+    d = make_d3D(eL.N, 4, mx);
+    c = make_d3D(eL.N, 4, mx);
+    xn = make_d3D(mx, dnm + 1, 3);
+    xm = make_d3D(mx, dnm + 1, 3);
+    Bp = make_d3D(nspc, 3, mx);
+    Wp = make_d4D(nspc, 3, mx, mx);
+    E = FRC_ANN_PARA(&R, &eL, e, d);
+    for (i = 0; i < eL.N; i++)
+        for (k = 0; k < 3; k++) f[3 * i + k] = ((eEFS == 1 || eEFS == 3) && eL.MRK[i]) ? eL.f[i][k] : 0.0;
+    for (int pass = 0; pass < 2; pass++) {
+        double *out = pass ? gF : gE;
+        int o = 0;
+        for (s = 0; s < nspc; s++)
+            for (k = 0; k < 3; k++)
+                for (m = 0; m < mx; m++) {
+                    Bp[s][k][m] = 0.0;
+                    for (n = 0; n < mx; n++) Wp[s][k][m][n] = 0.0;
+                }
+        if (pass == 0)
+            DE_ANN_PARA(&R, &eL, Bp, Wp, e);
+        else if (eEFS == 1 || eEFS == 3)
+            DF_ANN_PARA(&R, &eL, Bp, Wp, e, d, c, xn, xm);
+        for (s = 0; s < nspc; s++) {
+            for (k = 0; k < 3; k++)
+                for (m = 0; m < R.NU[k + 1]; m++) out[o++] = Bp[s][k][m];
+            for (k = 0; k < 3; k++)
+                for (m = 0; m < R.NU[k + 1]; m++)
+                    for (n = 0; n < R.NU[k]; n++) out[o++] = Wp[s][k][m][n];
+        }
+    }
+    free_d3D(e, eL.N, 4);
+    free_d3D(d, eL.N, 4);
+    free_d3D(c, eL.N, 4);
+    free_d3D(xn, mx, dnm + 1);
+    free_d3D(xm, mx, dnm + 1);
+    free_d3D(Bp, nspc, 3);
+    free_d4D(Wp, nspc, 3, mx);
+    free_d3D(R.B, nspc, 3);
+    free_d4D(R.W, nspc, 3, mx);
+    free_d2D(R.Rmin, nspc);
+    free_d2D(R.DR, nspc);
+    return E;
 }

@@ -102,6 +102,7 @@ def read_efile(path, D):
         for _ in range(NF):
             hdr = toks[li].split(); li += 1
             atom, dnn = int(hdr[0]), int(hdr[1])
+            F = np.array([float(v) for v in hdr[2:5]])
             Fn = np.zeros((dnn + 1, D, 3))
             for n in range(D):
                 Fn[dnn, n] = [float(v) for v in toks[li].split()]; li += 1
@@ -110,8 +111,8 @@ def read_efile(path, D):
                 dni.append(int(toks[li])); li += 1
                 for n in range(D):
                     Fn[j, n] = [float(v) for v in toks[li].split()]; li += 1
-            blocks.append((atom, np.array(dni, np.int32), Fn))
-    return G, atmn, marked, blocks
+            blocks.append((atom, np.array(dni, np.int32), Fn, F))
+    return G, atmn, marked, blocks, float(head[5])
 
 
 def make_parse():
@@ -125,18 +126,20 @@ def make_parse():
     out = dict(basis=open(os.path.join(base, "basis")).read(), spcz=np.array(species))
     names = sorted(k for k in index if os.path.exists(os.path.join(base, "ref", k)))
     lats, xs, ats, gs, offs = [], [], [], [], [0]
-    mk_atom, mk_struct, mk_dni, mk_fn = [], [], [], []
+    mk_atom, mk_struct, mk_dni, mk_fn, mk_F, E = [], [], [], [], [], []
     for s, name in enumerate(names):
         rel = index[name].replace("./", "")
         L, X, at = read_poscar(os.path.join(base, rel, "POSCAR.0"), species)
-        G, gat, marked, blocks = read_efile(os.path.join(base, "ref", name), 82)
+        G, gat, marked, blocks, e = read_efile(os.path.join(base, "ref", name), 82)
+        E.append(e)
         assert (gat == at).all(), name
         lats.append(L); xs.append(X); ats.append(at); gs.append(G); offs.append(offs[-1] + len(at))
-        for atom, dni, Fn in blocks:
-            mk_struct.append(s); mk_atom.append(atom); mk_dni.append(dni); mk_fn.append(Fn)
+        for atom, dni, Fn, F in blocks:
+            mk_struct.append(s); mk_atom.append(atom); mk_dni.append(dni); mk_fn.append(Fn); mk_F.append(F)
     out.update(names=np.array(names), lat=np.array(lats), x=np.concatenate(xs), atmn=np.concatenate(ats),
                G=np.concatenate(gs), offsets=np.array(offs), mk_struct=np.array(mk_struct),
-               mk_atom=np.array(mk_atom), mk_dni=np.array(mk_dni, dtype=object), mk_fn=np.array(mk_fn, dtype=object))
+               mk_atom=np.array(mk_atom), mk_dni=np.array(mk_dni, dtype=object), mk_fn=np.array(mk_fn, dtype=object),
+               mk_F=np.array(mk_F), E=np.array(E))
     np.savez_compressed(os.path.join(HERE, "parse_cuag.npz"), **out)
     print("parse:", len(names), "structures,", len(mk_atom), "marked atoms")
 
@@ -198,7 +201,6 @@ def make_ref_efs():
 
 
 if __name__ == "__main__":
-    make_parse()
-    make_kat()
-    make_relax()
-    make_ref_efs()
+    parts = {"parse": make_parse, "kat": make_kat, "relax": make_relax, "ref_efs": make_ref_efs}
+    for name in sys.argv[1:] or list(parts):
+        parts[name]()

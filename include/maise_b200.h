@@ -288,6 +288,12 @@ int mb_graphs(mb_potential *p, int enable);
 /* Start (enable=1) or stop timing of the fused descriptor/force kernel: every
  * launch is bracketed by CUDA events on the handle's stream (up to
  * `capacity` launches), and the kernel's pair/triplet counters are reset. */
+/* The autotuner's decisions so far: *count (at most cap) entries; entry k
+ * holds the pass mode (0 descriptors, 1 energy, 2 E/F/S, 3 VJP), whether the
+ * leg-table kernel ran (legs), the size bucket (N <= 2^bucket), the
+ * neighbour capacity, and the chosen shape (warps per atom, atoms per CTA). */
+int mb_tune_read(const mb_potential *pot, int cap, int *count, int *mode, int *legs, int *size_bucket, int *capacity,
+                 int *wpa, int *apb);
 int mb_profile(mb_potential *pot, int enable, int capacity);
 
 /* Synchronise and report: summed duration (ms) and number of timed launches

@@ -2261,6 +2261,16 @@ static int launch_leg_pass(const mb_dev *d, const mb_model *m, int shape, LegArg
     return rc;
 }
 
+/* warps per atom and atoms per CTA of shape `shape` of the leg kernel
+ * (legs != 0) or of k_efs */
+extern "C" int mbk_shape_dims(int legs, int shape, int *wpa, int *apb) {
+    if (shape < 0 || shape >= (legs ? MB_NLEGSHAPES : MB_NSHAPES)) return 1;
+    const EfsShape &e = legs ? kLegShapes[shape] : kShapes[shape];
+    *wpa = e.wpa;
+    *apb = e.apb;
+    return 0;
+}
+
 /* Autotuner: on the first pass of a (mode, size bucket, capacity) the three
  * shapes are each timed once (after an untimed launch) and the fastest is
  * kept for later passes of that key. */
@@ -2274,7 +2284,15 @@ static int tune_leg(mb_dev *d, const mb_model *m, int N, int mode, const LegArgs
     const int key = tune_key(d, N, mode);
     for (int k = 0; k < d->tune_n; k++)
         if (d->tune_key[k] == key) return d->tune_val[k];
-    if (d->tune_fixed >= 0) return d->tune_fixed < MB_NLEGSHAPES ? d->tune_fixed : 0;
+    if (d->tune_fixed >= 0) {
+        /* a forced shape is recorded as the decision for this key */
+        const int v = d->tune_fixed < MB_NLEGSHAPES ? d->tune_fixed : 0;
+        if (d->tune_n < MB_TUNE_SLOTS) {
+            d->tune_key[d->tune_n] = key;
+            d->tune_val[d->tune_n++] = v;
+        }
+        return v;
+    }
     LegArgs t = a;
     t.counters = nullptr;
     cudaEvent_t e0, e1;
@@ -2312,7 +2330,14 @@ static int tune_shape(mb_dev *d, const mb_model *m, int N, int mode, const EfsAr
     const int key = tune_key(d, N, mode);
     for (k = 0; k < d->tune_n; k++)
         if (d->tune_key[k] == key) return d->tune_val[k];
-    if (d->tune_fixed >= 0) return d->tune_fixed;
+    if (d->tune_fixed >= 0) {
+        const int v = d->tune_fixed < MB_NSHAPES ? d->tune_fixed : 0;
+        if (d->tune_n < MB_TUNE_SLOTS) {
+            d->tune_key[d->tune_n] = key;
+            d->tune_val[d->tune_n++] = v;
+        }
+        return v;
+    }
     EfsArgs t = a;
     t.counters = nullptr;
     cudaEvent_t e0, e1;

@@ -248,6 +248,23 @@ int mb_batch_stats(const mb_potential *p, long long *evals, double *ms) {
     return MB_OK;
 }
 
+int mb_tune_read(const mb_potential *p, int cap, int *count, int *mode, int *legs, int *size_bucket, int *capacity,
+                 int *wpa, int *apb) {
+    int k, n;
+    if (!p || cap < 0 || !count) return fail(MB_ERR_ARG, "bad arguments");
+    n = p->d.tune_n < cap ? p->d.tune_n : cap;
+    *count = n;
+    for (k = 0; k < n; k++) {
+        const int key = p->d.tune_key[k], lg = (key >> 26) & 1;
+        mode[k] = key >> 28;
+        legs[k] = lg;
+        size_bucket[k] = (key >> 20) & 0x3f;
+        capacity[k] = key & 0xfffff;
+        if (mbk_shape_dims(lg, p->d.tune_val[k], &wpa[k], &apb[k])) wpa[k] = apb[k] = 0;
+    }
+    return MB_OK;
+}
+
 int mb_profile(mb_potential *p, int enable, int capacity) {
     mb_dev *d;
     int k;

@@ -164,6 +164,7 @@ void mbk_record(void *event, void *stream);
 int mbk_shape_ready(const mb_dev *d, int N, int mode);
 int mbk_legs_model(const mb_model *m);
 int mbk_legs_usable(const mb_dev *d, const mb_model *m, int N, const mb_cell *c);
+int mbk_shape_dims(int legs, int shape, int *wpa, int *apb);
 int mbk_graph_cell_nodes(void *graph, void **nodes, int *rows, int cap);
 int mbk_graph_set_cell(void *exec, void *const *nodes, const int *rows, int count, const mb_cell *c, double pV);
 size_t mbk_efs_smem(const mb_model *m, int capNB, int shape);

@@ -85,3 +85,27 @@ def test_leg_path_every_shape(tmp_path, monkeypatch):
         pot.close()
         assert r["H"] == pytest.approx(want["H"], rel=1e-10), shape
         np.testing.assert_allclose(r["F"], want["F"], atol=1e-9, err_msg=str(shape))
+
+
+def test_tune_table_records_the_chosen_shapes(tmp_path, monkeypatch):
+    """The autotuner keeps one decision per (mode, kernel family, size
+    bucket, capacity) and the table reports it with the shape's dimensions."""
+    from maise_b200 import models
+
+    w = dict(_cases())["alloy"]
+    path = str(tmp_path / "model")
+    models.random_model(path, [29, 46, 47], models.Basis(), (w["X"], w["LAT"], w["atmn"], 3), seed=4)
+    legs, plain = _pots(monkeypatch, path)
+    for pot, uses_legs in ((legs, True), (plain, False)):
+        pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=300)
+        pot.energy(w["X"], w["LAT"], w["atmn"], ND=3, NM=300)
+        tt = pot.tune_table()
+        modes = {e["mode"] for e in tt}
+        assert {"efs", "energy"} <= modes
+        for e in tt:
+            assert e["legs"] == uses_legs
+            assert e["size_bucket"] == 8  # 256 atoms
+            assert e["wpa"] in (1, 2, 4, 8) and e["apb"] in (1, 2, 4)
+        n = len(tt)
+        pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=300)  # same key: no new decision
+        assert len(pot.tune_table()) == n

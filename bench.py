@@ -400,6 +400,7 @@ def config1_leg(local, td, peak, cpu=True):
     NM = 400
     pot = maise_b200.Potential(os.path.join(d, "model"), device=local)
     rate, k = _efs_rate(pot, w, 3, 2000, NM)
+    roof = _roofline(basis, 1, k, 32, peak, pot)  # before the relax adds its own tuner entries
     pot.relax(w["X"], w["LAT"], w["atmn"], ND=3, NM=NM, rlxt=3, mitr=5, etol=0.0)  # warm-up
     reps = 5
     t0 = time.perf_counter()
@@ -408,7 +409,7 @@ def config1_leg(local, td, peak, cpu=True):
     t_relax = (time.perf_counter() - t0) / reps
     out = {"workload": CFG1_WORKLOAD, "atoms": 32, "efs_atom_steps_per_s": rate,
            "model": "random weights with the binding sign structure (seed 1)",
-           "roofline": _roofline(basis, 1, k, 32, peak, pot), "relax_structures_per_s": 1.0 / t_relax,
+           "roofline": roof, "relax_structures_per_s": 1.0 / t_relax,
            "relax_iterations": r["iters"], "relax_H": r["H"], "relax_calls": [r["n_energy"], r["n_force"]]}
     pot.close()
     if cpu:
@@ -477,7 +478,8 @@ def particle_leg(local, td, peak, md_steps=500, cpu=True):
 
 def profile_case(case):
     """Small cases sized for an ncu capture (a few MB on the device):
-    md           the 4000-atom workload, 3 + 3 NVT steps (k_efs launches)
+    md           the 4000-atom workload: the bench's 20 settle steps, then 3 NVT
+                 steps at the settled neighbour counts (descriptor-pass launches)
     relax-batch  64 Mg-Ca structures of the population relax, 20 BFGS iterations
     surrogate    features of 512 Cu-Pd-Ag offspring and 5 training epochs"""
     import maise_b200
@@ -488,7 +490,7 @@ def profile_case(case):
         w, basis = workload()
         pot = maise_b200.Potential(make_model(td, w, basis))
         V = maxwell([atomic_mass(w["spcz"][s]) for s in w["atmn"]], 600.0, seed=7)
-        st = pot.md_nvt(w["X"], w["LAT"], w["atmn"], V, 600.0, nsteps=3, NM=100, trace=False)
+        st = pot.md_nvt(w["X"], w["LAT"], w["atmn"], V, 600.0, nsteps=SETTLE_STEPS, NM=100, trace=False)
         pot.md_nvt(st["X"], w["LAT"], w["atmn"], st["V"], 600.0, nsteps=3, NM=100, xi=st["xi"], trace=False)
     elif case == "relax-batch":
         pop = workloads.ea_population(count=64, seed=3)

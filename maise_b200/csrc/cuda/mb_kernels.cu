@@ -187,18 +187,43 @@ __global__ void k_cell_fill(int N, const int *cell_of, const int *start, int *cu
     atoms[start[k] + pos] = i;
 }
 
-/* order each cell's atoms by index so the neighbour order is deterministic */
+/* order each cell's atoms by index so the neighbour order is deterministic:
+ * one warp per cell, each atom placed at its rank (the number of smaller
+ * indices in the cell; indices are distinct); cells of more than
+ * 32 * CELL_SORT_PER_LANE atoms are sorted by one lane */
+#define CELL_SORT_PER_LANE 8
 __global__ void k_cell_sort(int ncell, const int *start, int *atoms) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (k >= ncell) return;
-    int lo = start[k], hi = start[k + 1];
-    for (int a = lo + 1; a < hi; a++) {
-        int v = atoms[a], b = a - 1;
-        while (b >= lo && atoms[b] > v) {
-            atoms[b + 1] = atoms[b];
-            b--;
+    const int lo = start[k], n = start[k + 1] - lo;
+    if (n <= 32 * CELL_SORT_PER_LANE) {
+        int v[CELL_SORT_PER_LANE], r[CELL_SORT_PER_LANE];
+#pragma unroll
+        for (int q = 0; q < CELL_SORT_PER_LANE; q++) {
+            const int e = q * 32 + lane;
+            v[q] = e < n ? atoms[lo + e] : 0x7fffffff;
+            r[q] = 0;
         }
-        atoms[b + 1] = v;
+        const int rounds = (n + 31) >> 5;
+        for (int f = 0; f < n; f++) {
+            const int w = atoms[lo + f];
+#pragma unroll
+            for (int q = 0; q < CELL_SORT_PER_LANE; q++)
+                if (q < rounds) r[q] += w < v[q];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < CELL_SORT_PER_LANE; q++)
+            if (q * 32 + lane < n) atoms[lo + r[q]] = v[q];
+    } else if (lane == 0) {
+        for (int a = lo + 1; a < lo + n; a++) {
+            int v = atoms[a], b = a - 1;
+            while (b >= lo && atoms[b] > v) {
+                atoms[b + 1] = atoms[b];
+                b--;
+            }
+            atoms[b + 1] = v;
+        }
     }
 }
 
@@ -1251,16 +1276,17 @@ struct LegArgs {
     int N, cap, mode;
     double urep;
     const int *nn, *nj, *nso;
-    const unsigned *nk;
     const double4 *nd;
     const double *leg;
+    const unsigned *trip; /* triplet lists (k_trip) */
+    const int *tboff;
+    int tcap;
     const int *spc;
     const mb_params *params;
     const double *weights;
     double *EA, *EU, *G, *F, *vir;
     unsigned long long *counters;
     size_t smem_group;
-    int tl_cap;
 };
 
 /* shared-memory carve-up of one atom group of k_efs_leg */
@@ -1269,30 +1295,23 @@ struct LegSmem {
     double *Fnb, *grid, *red, *h;           /* reductions, MLP, reverse pass   */
     double4 *d;
     double *ir, *L, *G;
-    double *tmp;                            /* G2 terms | */
-    unsigned *tl;                           /* triplet list */
-    uint2 *hash;
-    int *j, *sp, *jo, *blk, *seg;
-    unsigned *key;
+    double *tmp;                            /* G2 terms */
+    int *j, *sp, *seg;
 };
 
-__host__ __device__ inline size_t leg_smem_bytes(int cap, int D, int ng2, int warps, int tl) {
+__host__ __device__ inline size_t leg_smem_bytes(int cap, int D, int ng2, int warps) {
     size_t b = efs_union_bytes(cap, 64, warps, 1);
     b += sizeof(double4) * cap;
-    b += sizeof(double) * cap;                        /* ir */
-    b += sizeof(double) * cap * MB_LEG_STRIDE;        /* L */
-    b += align16(sizeof(double) * D);                 /* G */
-    const size_t tmp_b = sizeof(double) * cap * (ng2 > 1 ? ng2 : 1), tl_b = align16(sizeof(unsigned) * tl);
-    b += align16(tmp_b > tl_b ? tmp_b : tl_b);        /* tmp | tl */
-    b += sizeof(uint2) * LEG_HASH;
-    b += align16(sizeof(int) * cap) * 3;              /* j, sp, key */
-    b += sizeof(int) * 4 * cap;                       /* jo */
-    b += align16(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
-    b += sizeof(int) * 8;
+    b += sizeof(double) * cap;                                 /* ir */
+    b += sizeof(double) * cap * MB_LEG_STRIDE;                 /* L */
+    b += align16(sizeof(double) * D);                          /* G */
+    b += align16(sizeof(double) * cap * (ng2 > 1 ? ng2 : 1));  /* tmp */
+    b += align16(sizeof(int) * cap) * 2;                       /* j, sp */
+    b += sizeof(int) * 8;                                      /* seg */
     return align16(b);
 }
 
-__device__ inline LegSmem leg_carve(char *base, int cap, int D, int ng2, int warps, int tl) {
+__device__ inline LegSmem leg_carve(char *base, int cap, int D, int ng2, int warps) {
     LegSmem s;
     char *p = base;
     s.stage = (double *)p;
@@ -1305,103 +1324,157 @@ __device__ inline LegSmem leg_carve(char *base, int cap, int D, int ng2, int war
     s.ir = (double *)p; p += sizeof(double) * cap;
     s.L = (double *)p; p += sizeof(double) * cap * MB_LEG_STRIDE;
     s.G = (double *)p; p += align16(sizeof(double) * D);
-    {
-        const size_t tmp_b = sizeof(double) * cap * (ng2 > 1 ? ng2 : 1), tl_b = align16(sizeof(unsigned) * tl);
-        s.tmp = (double *)p;
-        s.tl = (unsigned *)p;
-        p += align16(tmp_b > tl_b ? tmp_b : tl_b);
-    }
-    s.hash = (uint2 *)p; p += sizeof(uint2) * LEG_HASH;
+    s.tmp = (double *)p; p += align16(sizeof(double) * cap * (ng2 > 1 ? ng2 : 1));
     s.j = (int *)p; p += align16(sizeof(int) * cap);
     s.sp = (int *)p; p += align16(sizeof(int) * cap);
-    s.key = (unsigned *)p; p += align16(sizeof(int) * cap);
-    s.jo = (int *)p; p += sizeof(int) * 4 * cap;
-    s.blk = (int *)p; p += align16(sizeof(int) * MB_MAX_BLOCKS * warps * 2);
     s.seg = (int *)p;
     return s;
 }
 
 __device__ __forceinline__ unsigned hash_slot(unsigned key) { return (key * 0x9E3779B1u) >> 24; }
 
-/* slot of the staged entry with this key, or -1 (linear probing, bounded) */
-__device__ __forceinline__ int hash_find(const LegSmem &s, unsigned key) {
-    unsigned h = hash_slot(key);
-    for (int probe = 0; probe < LEG_HASH; probe++) {
-        const uint2 e = s.hash[h];
-        if (e.x == key) return (int)e.y;
-        if (e.x == 0xffffffffu) return -1;
-        h = (h + 1u) & (LEG_HASH - 1u);
+/* start of species s in a list whose species starts are o (nso layout) */
+__device__ __forceinline__ int jo_at(const int4 &o, int s) { return s == 0 ? o.x : (s == 1 ? o.y : (s == 2 ? o.z : o.w)); }
+
+/* Triplet lists of the leg path: one warp per atom i, TRIP_WARPS atoms per
+ * CTA.  The warp stages i's entries in relative-species order (position u,
+ * the order k_efs_leg stages them in: relative species v holds absolute
+ * species (s0 + v) % ns) with each entry's key (atom << 15 | image), its
+ * atom j and the species starts of j's list, and puts the keys into a hash.
+ * For every species block (alpha <= beta) it then walks, for each entry a
+ * of relative species alpha, the entries c of j's own list whose atom has
+ * absolute species (s0 + beta) % ns, 32 candidates per round: the entry's
+ * atom k at image key(a) + key(c) is looked up among i's keys, and a found
+ * slot b > a makes (a, b) a triplet with r_ij, r_ik and r_jk below Rc
+ * (each (k, image) of j's list is a distinct image relative to i, so a
+ * pair (a, b) is found at most once and a list never exceeds
+ * tcap = cap (cap - 1) / 2).  Accepted entries a | b << 8 | c << 16 are
+ * written in candidate order (a ascending, then c), so every list is
+ * deterministic; tboff[8 i + blk] holds the start of each block and
+ * tboff[8 i + nblk] the end.  counters[1] (if set) receives the number of
+ * triplets. */
+#define TRIP_WARPS 8
+__global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tcap, int ns, const int *__restrict__ nn,
+                                                          const int *__restrict__ nj, const unsigned *__restrict__ nk,
+                                                          const int *__restrict__ nso, const int *__restrict__ spc,
+                                                          unsigned *__restrict__ trip, int *__restrict__ tboff,
+                                                          unsigned long long *counters) {
+    __shared__ uint2 hsh[TRIP_WARPS][LEG_HASH];
+    __shared__ int sj[TRIP_WARPS][MB_LEG_MAX_CAP];
+    __shared__ unsigned skey[TRIP_WARPS][MB_LEG_MAX_CAP];
+    __shared__ int4 sjo[TRIP_WARPS][MB_LEG_MAX_CAP];
+    __shared__ int sseg[TRIP_WARPS][8];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * TRIP_WARPS + w;
+    if (i >= N) return; /* whole warps; nothing below synchronises the CTA */
+    uint2 *hash = hsh[w];
+    int *js = sj[w], *seg = sseg[w];
+    unsigned *key = skey[w];
+    int4 *jo = sjo[w];
+    const int n = nn[i], s0 = spc[i];
+    const size_t row = (size_t)i * cap;
+    if (lane < 4) {
+        const int v = lane, sa = (s0 + v) % ns;
+        int c = 0, o = 0;
+        if (v < ns) c = nso[4 * i + sa + 1] - nso[4 * i + sa];
+        for (int u = 0; u < v; u++) {
+            const int su = (s0 + u) % ns;
+            o += nso[4 * i + su + 1] - nso[4 * i + su];
+        }
+        seg[v] = c;
+        seg[4 + v] = v < ns ? o : n;
     }
-    return -1;
-}
-
-/* Each lane's position (a, c) in the candidate legs of one species block:
- * for the staged neighbours a in [.., a_hi) of the block's first species,
- * the entries c of a's own list whose atom has absolute species sb. */
-struct LegCur {
-    int a, c;
-};
-
-__device__ __forceinline__ void leg_norm(const LegSmem &s, LegCur &u, int a_hi, int sb) {
-    while (u.a < a_hi) {
-        const int len = s.jo[4 * u.a + sb + 1] - s.jo[4 * u.a + sb];
-        if (u.c < len) break;
-        u.c -= len;
-        u.a++;
+    for (int t = lane; t < LEG_HASH; t += 32) hash[t] = make_uint2(0xffffffffu, 0u);
+    __syncwarp();
+    for (int u = lane; u < n; u += 32) {
+        int v = 0;
+        while (v + 1 < ns && u >= seg[4 + v + 1]) v++;
+        const int sa = (s0 + v) % ns;
+        const int t = nso[4 * i + sa] + (u - seg[4 + v]);
+        const int j = nj[row + t];
+        js[u] = j;
+        key[u] = nk[row + t];
+        jo[u] = *reinterpret_cast<const int4 *>(nso + 4 * (size_t)j);
     }
-}
-
-/* Append the block's accepted triplets (a, b, c) -- b > a, the entry c of
- * a's list being atom k at the image that puts it at i's slot b -- to this
- * warp's list region as a | b << 8 | c << 16, 32 candidates per round, the
- * warps of an atom taking every WPA-th round.  Stops when the region
- * cannot take another round; returns 1 once the block is exhausted. */
-template <int WPA>
-__device__ __forceinline__ int leg_fill(const LegSmem &s, const unsigned *__restrict__ nk, int cap, int a_hi, int sb,
-                                        LegCur &u, int &pos, int hi, int lane) {
-    for (;;) {
-        const bool live = u.a < a_hi;
-        if (!__any_sync(FULL, live)) return 1;
-        if (pos + 32 > hi) return 0;
-        bool ok = false;
-        unsigned ent = 0u;
-        if (live) {
-            const int a = u.a, c = s.jo[4 * a + sb] + u.c;
-            const unsigned kc = __ldg(nk + (size_t)s.j[a] * cap + c), ka = s.key[a];
-            const int x0 = sx5(ka >> 10) + sx5(kc >> 10), x1 = sx5(ka >> 5) + sx5(kc >> 5), x2 = sx5(ka) + sx5(kc);
-            if (x0 >= -16 && x0 <= 15 && x1 >= -16 && x1 <= 15 && x2 >= -16 && x2 <= 15) {
-                const unsigned key =
-                    (kc & ~0x7fffu) | (((unsigned)x0 & 31u) << 10) | (((unsigned)x1 & 31u) << 5) | ((unsigned)x2 & 31u);
-                const int b = hash_find(s, key);
-                ok = b > a;
-                ent = (unsigned)a | ((unsigned)b << 8) | ((unsigned)c << 16);
+    __syncwarp();
+    for (int u = lane; u < n; u += 32) {
+        const unsigned k = key[u];
+        unsigned h = hash_slot(k);
+        for (int probe = 0; probe < LEG_HASH; probe++) {
+            if (atomicCAS(&hash[h].x, 0xffffffffu, k) == 0xffffffffu) {
+                hash[h].y = (unsigned)u;
+                break;
+            }
+            h = (h + 1u) & (LEG_HASH - 1u);
+        }
+    }
+    __syncwarp();
+    unsigned *out = trip + (size_t)i * tcap;
+    int pos = 0, blkid = 0;
+    for (int al = 0; al < ns; al++)
+        for (int be = al; be < ns; be++, blkid++) {
+            if (lane == 0) tboff[8 * i + blkid] = pos;
+            const int sb = (s0 + be) % ns, a_hi = seg[4 + al] + seg[al];
+            int ca = seg[4 + al], cc = lane;
+            /* the lane's candidate (ca, cc): entry cc of species sb in the list of i's entry ca */
+            auto norm = [&]() {
+                while (ca < a_hi) {
+                    const int4 o = jo[ca];
+                    const int len = jo_at(o, sb + 1) - jo_at(o, sb);
+                    if (cc < len) break;
+                    cc -= len;
+                    ca++;
+                }
+            };
+            norm();
+            for (;;) {
+                const bool live = ca < a_hi;
+                if (!__any_sync(FULL, live)) break;
+                bool ok = false;
+                unsigned ent = 0u;
+                if (live) {
+                    const int c = jo_at(jo[ca], sb) + cc;
+                    const unsigned kc = __ldg(nk + (size_t)js[ca] * cap + c), ka = key[ca];
+                    const int x0 = sx5(ka >> 10) + sx5(kc >> 10), x1 = sx5(ka >> 5) + sx5(kc >> 5),
+                              x2 = sx5(ka) + sx5(kc);
+                    if (x0 >= -16 && x0 <= 15 && x1 >= -16 && x1 <= 15 && x2 >= -16 && x2 <= 15) {
+                        const unsigned kk = (kc & ~0x7fffu) | (((unsigned)x0 & 31u) << 10) |
+                                            (((unsigned)x1 & 31u) << 5) | ((unsigned)x2 & 31u);
+                        unsigned h = hash_slot(kk);
+                        int b = -1;
+                        for (int probe = 0; probe < LEG_HASH; probe++) {
+                            const uint2 e = hash[h];
+                            if (e.x == kk) {
+                                b = (int)e.y;
+                                break;
+                            }
+                            if (e.x == 0xffffffffu) break;
+                            h = (h + 1u) & (LEG_HASH - 1u);
+                        }
+                        ok = b > ca;
+                        ent = (unsigned)ca | ((unsigned)b << 8) | ((unsigned)c << 16);
+                    }
+                }
+                const unsigned m = __ballot_sync(FULL, ok);
+                if (ok) out[pos + __popc(m & ((1u << lane) - 1u))] = ent;
+                pos += __popc(m);
+                cc += 32;
+                norm();
             }
         }
-        const unsigned m = __ballot_sync(FULL, ok);
-        if (ok) s.tl[pos + __popc(m & ((1u << lane) - 1u))] = ent;
-        pos += __popc(m);
-        u.c += 32 * WPA;
-        leg_norm(s, u, a_hi, sb);
+    if (lane == 0) {
+        tboff[8 * i + blkid] = pos;
+        if (counters) atomicAdd(&counters[1], (unsigned long long)pos);
     }
 }
 
-/* body(ent, valid) over list entries [from, to) with the warp converged */
+/* body(ent) -> the entry's force on neighbour a, over list entries
+ * [from, to): each lane takes a contiguous run of K entries (K odd);
+ * consecutive entries mostly share a, so the a-side forces are summed in
+ * registers and added to Fnb once per change of a. */
 template <class Body>
-__device__ __forceinline__ void leg_run_all(const LegSmem &s, int from, int to, int lane, Body body) {
-    for (int base = from; base < to; base += 32) {
-        const int t = base + lane;
-        const bool valid = t < to;
-        body(valid ? s.tl[t] : 0u, valid);
-    }
-}
-
-/* body(ent) -> the entry's force on neighbour a, over entries [from, to):
- * each lane takes a contiguous run of K entries (K odd, so that the lanes'
- * list reads fall in distinct banks); consecutive entries mostly share a,
- * so the a-side forces are summed in registers and added to Fnb once per
- * change of a. */
-template <class Body>
-__device__ __forceinline__ void leg_run_runs(const LegSmem &s, int from, int to, int lane, Body body) {
+__device__ __forceinline__ void leg_run_runs(const LegSmem &s, const unsigned *__restrict__ list, int from, int to,
+                                             int lane, Body body) {
     int K = (to - from + 31) >> 5;
     if (K > 0) K |= 1;
     const int t0 = from + lane * K;
@@ -1410,7 +1483,7 @@ __device__ __forceinline__ void leg_run_runs(const LegSmem &s, int from, int to,
     for (int step = 0; step < K; step++) {
         const int t = t0 + step;
         if (t >= to) break;
-        const unsigned ent = s.tl[t];
+        const unsigned ent = __ldg(list + t);
         const int a = (int)(ent & 0xffu);
         if (a != ca) {
             if (ca >= 0) {
@@ -1433,47 +1506,11 @@ __device__ __forceinline__ void leg_run_runs(const LegSmem &s, int from, int to,
     }
 }
 
-/* Enumerate block (alpha, beta) for this warp and run `body` over its
- * triplets: from the stored entries [blk[0], blk[1]) when `reuse`, else
- * filling the region (in rounds when it overflows).  Records the range and
- * returns 0 if the region overflowed (the range is then not reusable). */
-template <int WPA, int RUN, class Body>
-__device__ __forceinline__ int leg_block(const LegSmem &s, const unsigned *__restrict__ nk, int cap, int a_lo, int a_hi,
-                                         int sb, int *blk, int reuse, int &pos, int lo, int hi, int warp, int lane,
-                                         Body body) {
-    if (reuse) {
-        if constexpr (RUN == RUN_CONVERGED)
-            leg_run_all(s, blk[0], blk[1], lane, body);
-        else
-            leg_run_runs(s, blk[0], blk[1], lane, body);
-        return 1;
-    }
-    LegCur u{a_lo, warp * 32 + lane};
-    leg_norm(s, u, a_hi, sb);
-    int start = pos, whole = 1;
-    for (;;) {
-        const int from = pos;
-        const int done = leg_fill<WPA>(s, nk, cap, a_hi, sb, u, pos, hi, lane);
-        __syncwarp();
-        if constexpr (RUN == RUN_CONVERGED)
-            leg_run_all(s, from, pos, lane, body);
-        else
-            leg_run_runs(s, from, pos, lane, body);
-        __syncwarp();
-        if (done) break;
-        whole = 0; /* region full: restart it for the next round */
-        start = pos = lo;
-    }
-    blk[0] = start;
-    blk[1] = pos;
-    return whole;
-}
-
 /* The fused descriptor / MLP / force kernel on leg tables: the stages of
- * k_efs with every triplet's leg factors read from the rows k_legs wrote
- * (i-j and i-k from i's own rows, staged; j-k from j's row in global
- * memory, L2-resident).  Reference bases: at most 8 G4 exponents, zeta in
- * {1, 2, 4, 16} or other integers, 2 lambdas. */
+ * k_efs over the triplet lists of k_trip, with every triplet's leg factors
+ * read from the rows k_legs wrote (i-j and i-k from i's own rows, staged;
+ * j-k from j's row in global memory, L2-resident).  Reference bases: at
+ * most 8 G4 exponents, zeta in {1, 2, 4, 16} or other integers, 2 lambdas. */
 template <int NE, int WPA, int APB>
 __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
     constexpr int NZ = 4, NLAM = 2, NZL = 8;
@@ -1492,9 +1529,9 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
     const int i = blockIdx.x * APB + group;
     if (i >= A.N) return; /* whole atom groups only: no barrier spans two groups */
     const int D = P.D, ns = P.nspc, ng2 = P.ng2, ne = P.ne, cap = A.cap;
-    LegSmem s = leg_carve(smem_raw + (size_t)group * A.smem_group, cap, D, ng2, WPA, A.tl_cap);
-    const int tlw = A.tl_cap / WPA, tl_lo = warp * tlw, tl_hi = tl_lo + tlw;
-    int tl_pos = tl_lo, tl_whole = 1;
+    LegSmem s = leg_carve(smem_raw + (size_t)group * A.smem_group, cap, D, ng2, WPA);
+    const unsigned *tl = A.trip + (size_t)i * A.tcap;
+    const int *tb = A.tboff + 8 * (size_t)i;
     const int n = A.nn[i];
     const int s0 = A.spc[i];
     const double *net = A.weights + P.w_off[s0];
@@ -1514,7 +1551,6 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
         s.seg[4 + v] = v < ns ? o : n;
     }
     for (int t = tid; t < D; t += NT) s.G[t] = 0.0;
-    for (int t = tid; t < LEG_HASH; t += NT) s.hash[t] = make_uint2(0xffffffffu, 0u);
     group_sync<WPA>();
     for (int u = tid; u < n; u += NT) {
         int v = 0;
@@ -1525,30 +1561,12 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
         const double4 dv = A.nd[row + t];
         s.j[u] = j;
         s.sp[u] = sa;
-        s.key[u] = A.nk[row + t];
         s.d[u] = dv;
         s.ir[u] = 1.0 / dv.w;
         const double2 *src = reinterpret_cast<const double2 *>(A.leg + (row + t) * MB_LEG_STRIDE);
         double2 *dst = reinterpret_cast<double2 *>(s.L + (size_t)u * MB_LEG_STRIDE);
 #pragma unroll
         for (int k = 0; k < MB_LEG_STRIDE / 2; k++) dst[k] = __ldg(src + k);
-        const int4 jo = *reinterpret_cast<const int4 *>(A.nso + 4 * j);
-        s.jo[4 * u] = jo.x;
-        s.jo[4 * u + 1] = jo.y;
-        s.jo[4 * u + 2] = jo.z;
-        s.jo[4 * u + 3] = jo.w;
-    }
-    group_sync<WPA>();
-    for (int u = tid; u < n; u += NT) {
-        const unsigned key = s.key[u];
-        unsigned h = hash_slot(key);
-        for (int probe = 0; probe < LEG_HASH; probe++) {
-            if (atomicCAS(&s.hash[h].x, 0xffffffffu, key) == 0xffffffffu) {
-                s.hash[h].y = (unsigned)u;
-                break;
-            }
-            h = (h + 1u) & (LEG_HASH - 1u);
-        }
     }
     group_sync<WPA>();
     if (tid == 0 && A.counters) atomicAdd(&A.counters[0], (unsigned long long)n);
@@ -1583,10 +1601,8 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
 
         /* ---- forward triplet terms, block by block, on the FP64 tensor cores ---- */
         int blkid = 0;
-        unsigned long long nacc = 0;
         for (int al = 0; al < ns; al++)
             for (int be = al; be < ns; be++, blkid++) {
-                const int sb = (s0 + be) % ns;
                 double c0 = 0.0, c1 = 0.0;
                 double *stw = s.stage + warp * 32 * EFS_STG;
                 auto body = [&](unsigned ent, bool valid) {
@@ -1596,7 +1612,6 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
 #pragma unroll
                     for (int q = 0; q < NZL; q++) lz[q] = 0.0;
                     if (valid) {
-                        nacc++;
                         const int a = (int)(ent & 0xffu), b = (int)((ent >> 8) & 0xffu), cj = (int)(ent >> 16);
                         const double4 d1 = s.d[a], d2 = s.d[b];
                         const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (s.ir[a] * s.ir[b]);
@@ -1627,10 +1642,11 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
                     }
                     __syncwarp();
                 };
-                int *blk = s.blk + (blkid * WPA + warp) * 2;
-                const int a_lo = s.seg[4 + al], a_hi = a_lo + s.seg[al];
-                tl_whole &= leg_block<WPA, RUN_CONVERGED>(s, A.nk, cap, a_lo, a_hi, sb, blk, 0, tl_pos, tl_lo,
-                                                          tl_hi, warp, lane, body);
+                /* the block's list entries, 32 per round, the atom's warps taking every WPA-th round */
+                for (int base = tb[blkid] + warp * 32, to = tb[blkid + 1]; base < to; base += 32 * WPA) {
+                    const int t = base + lane;
+                    body(t < to ? __ldg(tl + t) : 0u, t < to);
+                }
                 group_sync<WPA>();
                 group_store64<WPA>(c0, c1, s, warp, lane);
                 {
@@ -1640,10 +1656,6 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
                 }
                 group_sync<WPA>();
             }
-        if (A.counters) {
-            for (int o = 16; o > 0; o >>= 1) nacc += __shfl_xor_sync(FULL, nacc, o);
-            if (lane == 0) atomicAdd(&A.counters[1], nacc);
-        }
         if (A.mode == MB_MODE_DESCRIPTORS) {
             for (int t = tid; t < D; t += NT) A.G[(size_t)i * D + t] = s.G[t];
             return;
@@ -1728,17 +1740,14 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
     }
     group_sync<WPA>();
 
-    /* ---- reverse triplet terms (the forward list reused) ---- */
+    /* ---- reverse triplet terms over the same lists ---- */
     {
-        const int reuse = (A.mode != MB_MODE_VJP) && tl_whole;
         int blkid = 0;
-        tl_pos = tl_lo;
         double eta[NE];
 #pragma unroll
         for (int e = 0; e < NE; e++) eta[e] = e < ne ? P.d_eta4[e] : 0.0;
         for (int al = 0; al < ns; al++)
             for (int be = al; be < ns; be++, blkid++) {
-                const int sb = (s0 + be) % ns;
                 const int base = P.ind4[al * al + be * be];
                 for (int t = tid; t < 64; t += NT) s.grid[t] = 0.0;
                 group_sync<WPA>();
@@ -1801,10 +1810,12 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
                     atomicAdd(&s.Fnb[3 * b + 2], -g2z);
                     return make_double3(g1x, g1y, g1z);
                 };
-                int *blk = s.blk + (blkid * WPA + warp) * 2;
-                const int a_lo = s.seg[4 + al], a_hi = a_lo + s.seg[al];
-                leg_block<WPA, RUN_RUNS>(s, A.nk, cap, a_lo, a_hi, sb, blk, reuse, tl_pos, tl_lo, tl_hi, warp, lane,
-                                         body);
+                {
+                    /* the block's entries in WPA contiguous parts, one per warp */
+                    const int from = tb[blkid], to = tb[blkid + 1], per = (to - from + WPA - 1) / WPA;
+                    const int lo = min(to, from + warp * per), hi = min(to, lo + per);
+                    leg_run_runs(s, tl, lo, hi, lane, body);
+                }
                 group_sync<WPA>();
             }
     }
@@ -1964,63 +1975,112 @@ __global__ void __launch_bounds__(32) k_jvp(JvpArgs A) {
 /* reductions                                                          */
 /* ------------------------------------------------------------------ */
 
-/* out[0]=E, out[1]=H, out[2..7]=U; fixed-order block reduction */
-__global__ void k_finalize(int N, int mode, double pV, const double *EA, const double *EU, const double *vir,
-                           double *F, double *out) {
+/* Atoms per CTA of the multi-CTA reductions: chunks of at least 512 atoms,
+ * at most MB_RED_MAXB CTAs; nparts = 0 runs one CTA over all atoms. */
+__host__ __device__ inline int red_chunk(int N, int nparts) {
+    if (nparts <= 0) return N > 0 ? N : 1;
+    const int c = (N + MB_RED_MAXB - 1) / MB_RED_MAXB;
+    return c > 512 ? c : 512;
+}
+
+/* Sum of acc[0..K-1] over the CTA's 256 threads (fixed tree) into red[k][0]. */
+template <int K>
+__device__ __forceinline__ void block_tree(double (*red)[256], const double *acc, int t) {
+    for (int k = 0; k < K; k++) red[k][t] = acc[k];
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (t < h)
+            for (int k = 0; k < K; k++) red[k][t] += red[k][t + h];
+        __syncthreads();
+    }
+}
+
+/* After block_tree: CTA partials go to part[cta][0..K-1]; returns true in
+ * thread 0 of the CTA that finished last, which then holds the sums of the
+ * partials in CTA order in tot[] (and has reset the ticket). */
+template <int K>
+__device__ __forceinline__ bool last_cta(double (*red)[256], double *part, unsigned *ticket, double *tot, int t) {
+    __shared__ bool is_last;
+    const int nb = gridDim.x;
+    if (nb == 1) {
+        if (t == 0)
+            for (int k = 0; k < K; k++) tot[k] = red[k][0];
+        return t == 0;
+    }
+    if (t == 0) {
+        for (int k = 0; k < K; k++) part[blockIdx.x * 8 + k] = red[k][0];
+        __threadfence();
+        is_last = atomicAdd(ticket, 1u) == (unsigned)(nb - 1);
+    }
+    __syncthreads();
+    if (!is_last || t != 0) return false;
+    __threadfence();
+    const volatile double *vp = part;
+    for (int k = 0; k < K; k++) {
+        double s = 0.0;
+        for (int c = 0; c < nb; c++) s += vp[c * 8 + k];
+        tot[k] = s;
+    }
+    *ticket = 0u;
+    return true;
+}
+
+/* out[0]=E, out[1]=H, out[2..7]=U: every CTA reduces a fixed chunk of atoms
+ * (threads strided, then a tree) and zeroes the chunk's force components
+ * below 1e-8 (src/cmod.c:177-184); the last CTA adds the partials in CTA
+ * order.  Every sum has a fixed order, so results are reproducible. */
+__global__ void __launch_bounds__(256) k_finalize(int N, int mode, double pV, const double *EA, const double *EU,
+                                                  const double *vir, double *F, double *out, double *part,
+                                                  unsigned *ticket) {
     __shared__ double red[7][256];
-    int t = threadIdx.x;
+    const int t = threadIdx.x, chunk = red_chunk(N, part ? 1 : 0);
+    const int lo = blockIdx.x * chunk, hi = min(N, lo + chunk);
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int i = t; i < N; i += 256) {
+    for (int i = lo + t; i < hi; i += 256) {
         acc[0] += EA[i] + EU[i];
         if (mode != MB_MODE_ENERGY)
             for (int k = 0; k < 6; k++) acc[1 + k] += vir[(size_t)i * 6 + k];
     }
-    for (int k = 0; k < 7; k++) red[k][t] = acc[k];
-    __syncthreads();
-    for (int h = 128; h > 0; h >>= 1) {
-        if (t < h)
-            for (int k = 0; k < 7; k++) red[k][t] += red[k][t + h];
-        __syncthreads();
-    }
-    if (t == 0) {
-        out[0] = red[0][0];
-        out[1] = red[0][0] + pV;
+    if (mode == MB_MODE_EFS)
+        for (int i = 3 * lo + t; i < 3 * hi; i += 256)
+            if (fabs(F[i]) < 1e-8) F[i] = 0.0;
+    block_tree<7>(red, acc, t);
+    double tot[7];
+    if (last_cta<7>(red, part, ticket, tot, t)) {
+        out[0] = tot[0];
+        out[1] = tot[0] + pV;
         for (int k = 0; k < 6; k++) {
-            double u = red[1 + k][0];
+            double u = tot[1 + k];
             if (mode == MB_MODE_EFS && fabs(u) < 1e-8) u = 0.0;
             out[2 + k] = u;
         }
     }
-    if (mode == MB_MODE_EFS)
-        for (int i = t; i < 3 * N; i += 256)
-            if (fabs(F[i]) < 1e-8) F[i] = 0.0;
 }
 
 /* ------------------------------------------------------------------ */
 /* NVT step (src/cmod.c:403-407, 440-453)                              */
 /* ------------------------------------------------------------------ */
 
-/* K = 1/2 sum m v^2 in atom order, then xi += dt/tau^2 (2K/(3NT) - 1).
- * out[8] = K, out[9] = xi; trace[2*step] = H, trace[2*step+1] = K with the
- * step index kept in out[10] and advanced here, so that a captured chunk of
- * steps can be replayed unchanged. */
-__global__ void k_nvt_thermostat(int N, const double *V, const int *spc, const double *mass, double dt, double tau,
-                                 double T, double *out, double *trace, int capTrace) {
-    __shared__ double red[256];
-    int t = threadIdx.x;
-    double k = 0.0;
-    for (int i = t; i < N; i += 256) {
+/* K = 1/2 sum m v^2 (CTA chunks, then the partials in CTA order), then
+ * xi += dt/tau^2 (2K/(3NT) - 1).  out[8] = K, out[9] = xi;
+ * trace[2*step] = H, trace[2*step+1] = K with the step index kept in
+ * out[10] and advanced here, so that a captured chunk of steps can be
+ * replayed unchanged. */
+__global__ void __launch_bounds__(256) k_nvt_thermostat(int N, const double *V, const int *spc, const double *mass,
+                                                        double dt, double tau, double T, double *out, double *trace,
+                                                        int capTrace, double *part, unsigned *ticket) {
+    __shared__ double red[1][256];
+    const int t = threadIdx.x, chunk = red_chunk(N, part ? 1 : 0);
+    const int lo = blockIdx.x * chunk, hi = min(N, lo + chunk);
+    double k[1] = {0.0};
+    for (int i = lo + t; i < hi; i += 256) {
         double m = mass[spc[i]];
-        k += m * V[3 * i] * V[3 * i] + m * V[3 * i + 1] * V[3 * i + 1] + m * V[3 * i + 2] * V[3 * i + 2];
+        k[0] += m * V[3 * i] * V[3 * i] + m * V[3 * i + 1] * V[3 * i + 1] + m * V[3 * i + 2] * V[3 * i + 2];
     }
-    red[t] = k;
-    __syncthreads();
-    for (int h = 128; h > 0; h >>= 1) {
-        if (t < h) red[t] += red[t + h];
-        __syncthreads();
-    }
-    if (t == 0) {
-        double K = 0.5 * red[0];
+    block_tree<1>(red, k, t);
+    double tot[1];
+    if (last_cta<1>(red, part, ticket, tot, t)) {
+        double K = 0.5 * tot[0];
         double fs = 1.0 / (tau * tau) * (2.0 * K / ((3.0 * (double)N) * T) - 1.0);
         const int step = (int)out[10];
         out[8] = K;
@@ -2193,7 +2253,7 @@ extern "C" int mbk_legs_model(const mb_model *m) { return leg_model_ok(m) ? 1 : 
  * qualifies, the tables are allocated, and every entry key fits (atom
  * index in 17 bits, images within +-15, neighbour capacity <= 128) */
 extern "C" int mbk_legs_usable(const mb_dev *d, const mb_model *m, int N, const mb_cell *c) {
-    if (!d->nk || !d->leg || !d->nso) return 0;
+    if (!d->nk || !d->leg || !d->nso || !d->trip || !d->tboff) return 0;
     if (N >= MB_LEG_MAX_ATOMS || d->capNB > MB_LEG_MAX_CAP) return 0;
     for (int q = 0; q < 3; q++)
         if (c->Nq[q] > MB_LEG_MAX_IMAGE) return 0;
@@ -2203,17 +2263,8 @@ extern "C" int mbk_legs_usable(const mb_dev *d, const mb_model *m, int N, const 
 static const EfsShape kLegShapes[] = {{1, 4}, {1, 2}, {2, 1}, {4, 1}};
 #define MB_NLEGSHAPES 4
 
-/* triplet-list entries per atom group: 1536 per warp for one warp per atom
- * (about 930 triplets per atom in the dense alloy), 1024 per warp otherwise,
- * never more than there are candidate pairs */
-static int tl_entries_leg(int capNB, int wpa) {
-    const int all = capNB * (capNB - 1) / 2 + 32 * wpa;
-    const int v = wpa * (wpa == 1 ? 1536 : 1024);
-    return v < all ? v : all;
-}
-
 static size_t leg_group_bytes(const mb_model *m, int capNB, int wpa) {
-    return leg_smem_bytes(capNB, m->P.D, m->P.ng2, wpa, tl_entries_leg(capNB, wpa));
+    return leg_smem_bytes(capNB, m->P.D, m->P.ng2, wpa);
 }
 
 template <int NE, int WPA, int APB>
@@ -2233,14 +2284,15 @@ static int launch_leg(const LegArgs &a, cudaStream_t st) {
     return (int)cudaGetLastError();
 }
 
-/* k_legs then k_efs_leg in shape `shape`; the events (if any) bracket both */
+/* k_legs, k_trip, then k_efs_leg in shape `shape`; the events (if any) bracket the three */
 static int launch_leg_pass(const mb_dev *d, const mb_model *m, int shape, LegArgs a, cudaStream_t st, cudaEvent_t e0,
                            cudaEvent_t e1) {
     a.smem_group = leg_group_bytes(m, a.cap, kLegShapes[shape].wpa);
-    a.tl_cap = tl_entries_leg(a.cap, kLegShapes[shape].wpa);
     if (e0) mbk_record(e0, st);
     k_legs<<<(a.N + 3) / 4, 128, 0, st>>>(a.N, a.cap, d->nn, d->nj, d->nk, (double4 *)d->nd, d->spc, d->params,
                                          d->leg, d->nso);
+    k_trip<<<(a.N + TRIP_WARPS - 1) / TRIP_WARPS, 32 * TRIP_WARPS, 0, st>>>(
+        a.N, a.cap, d->tcap, m->P.nspc, d->nn, d->nj, d->nk, d->nso, d->spc, d->trip, d->tboff, a.counters);
     int rc;
     if (m->P.ne <= 7) {
         switch (shape) {
@@ -2402,8 +2454,10 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
         la.nn = d->nn;
         la.nj = d->nj;
         la.nso = d->nso;
-        la.nk = d->nk;
         la.nd = (const double4 *)d->nd;
+        la.trip = d->trip;
+        la.tboff = d->tboff;
+        la.tcap = d->tcap;
         la.leg = d->leg;
         la.spc = d->spc;
         la.params = d->params;
@@ -2415,7 +2469,6 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
         la.vir = d->vir;
         la.counters = d->counters;
         la.smem_group = 0;
-        la.tl_cap = 0;
         const int shape = tune_leg(d, m, N, mode, la, st);
         d->last_shape = 16 + shape;
         cudaEvent_t e0 = 0, e1 = 0;
@@ -2426,7 +2479,7 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
         }
         if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
         const int rc = launch_leg_pass(d, m, shape, la, st, e0, e1);
-        (*launches) += 2;
+        (*launches) += 3;
         return rc;
     }
     int shape = tune_shape(d, m, N, mode, a, st);
@@ -2472,7 +2525,9 @@ extern "C" int mbk_jvp(mb_dev *d, const mb_model *m, int N, const double *dx, co
 }
 
 extern "C" int mbk_finalize(mb_dev *d, int N, int mode, double pV, void *stream, long *launches) {
-    k_finalize<<<1, 256, 0, (cudaStream_t)stream>>>(N, mode, pV, d->EA, d->EU, d->vir, d->F, d->out);
+    const int chunk = red_chunk(N, d->part ? 1 : 0), nb = (N + chunk - 1) / chunk;
+    k_finalize<<<nb > 0 ? nb : 1, 256, 0, (cudaStream_t)stream>>>(N, mode, pV, d->EA, d->EU, d->vir, d->F, d->out,
+                                                                   d->part, d->ticket);
     (*launches)++;
     return (int)cudaGetLastError();
 }
@@ -2483,7 +2538,10 @@ extern "C" int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, do
     (void)m;
     /* masses by species live after the weights in the parameter upload (see mb_core.c) */
     const double *mass = d->weights + m->weights_len;
-    k_nvt_thermostat<<<1, 256, 0, st>>>(N, d->V, d->spc, mass, dt, tau, T, d->out, d->trace, d->capTrace);
+    const int chunk = red_chunk(N, d->part ? 1 : 0), nb = (N + chunk - 1) / chunk;
+    k_nvt_thermostat<<<nb > 0 ? nb : 1, 256, 0, st>>>(N, d->V, d->spc, mass, dt, tau, T, d->out, d->trace,
+                                                      d->capTrace, d->part ? d->part + MB_RED_MAXB * 8 : nullptr,
+                                                      d->ticket ? d->ticket + 1 : nullptr);
     k_nvt_integrate<<<(N + 127) / 128, 128, 0, st>>>(N, d->X, d->V, d->F, d->spc, mass, dt, d->out);
     *launches += 2;
     return (int)cudaGetLastError();

@@ -161,6 +161,9 @@ int mb_open(const char *model_path, int device, mb_potential **out) {
        "upload masses");
     CK(cudaMalloc((void **)&p->d.out, sizeof(double) * 16), "cudaMalloc out");
     CK(cudaMemset(p->d.out, 0, sizeof(double) * 16), "memset out");
+    CK(cudaMalloc((void **)&p->d.part, sizeof(double) * 2 * MB_RED_MAXB * 8), "cudaMalloc part");
+    CK(cudaMalloc((void **)&p->d.ticket, sizeof(unsigned) * 2), "cudaMalloc ticket");
+    CK(cudaMemset(p->d.ticket, 0, sizeof(unsigned) * 2), "memset ticket");
     CK(cudaMalloc((void **)&p->d.status, sizeof(int) * 4), "cudaMalloc status");
     CK(cudaMalloc((void **)&p->d.counters, sizeof(unsigned long long) * 2), "cudaMalloc counters");
     CK(cudaMemset(p->d.counters, 0, sizeof(unsigned long long) * 2), "memset counters");
@@ -172,7 +175,7 @@ int mb_open(const char *model_path, int device, mb_potential **out) {
 }
 
 static void dev_free(mb_dev *d) {
-    cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso);
+    cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso); cudaFree(d->trip); cudaFree(d->tboff);
     cudaFree(d->X); cudaFree(d->V); cudaFree(d->spc); cudaFree(d->nn); cudaFree(d->nj); cudaFree(d->nd);
     cudaFree(d->F); cudaFree(d->EA); cudaFree(d->EU); cudaFree(d->vir); cudaFree(d->G);
     cudaFree(d->cell_of); cudaFree(d->cell_cnt); cudaFree(d->cell_start); cudaFree(d->cell_atoms);
@@ -196,6 +199,8 @@ int mb_close(mb_potential *p) {
     cudaFree(p->d.params);
     cudaFree(p->d.weights);
     cudaFree(p->d.out);
+    cudaFree(p->d.part);
+    cudaFree(p->d.ticket);
     cudaFree(p->d.status);
     cudaFree(p->d.counters);
     cudaFree(p->d.flush);
@@ -391,14 +396,16 @@ static int ensure(mb_potential *p, int N, int nb, int ncell) {
         d->capN = cap;
         p->gen++;
         cudaFree(d->nj); cudaFree(d->nd); cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso);
-        d->nj = NULL; d->nd = NULL; d->nk = NULL; d->leg = NULL; d->nso = NULL;
+        cudaFree(d->trip); cudaFree(d->tboff);
+        d->nj = NULL; d->nd = NULL; d->nk = NULL; d->leg = NULL; d->nso = NULL; d->trip = NULL; d->tboff = NULL;
         d->capNB = 0;
     }
     if (nb > d->capNB || !d->nj) {
         int cap = nb > d->capNB ? nb : d->capNB;
         cap = (cap + 7) & ~7;
         cudaFree(d->nj); cudaFree(d->nd); cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso);
-        d->nk = NULL; d->leg = NULL; d->nso = NULL;
+        cudaFree(d->trip); cudaFree(d->tboff);
+        d->nk = NULL; d->leg = NULL; d->nso = NULL; d->trip = NULL; d->tboff = NULL;
         CK(cudaMalloc((void **)&d->nj, sizeof(int) * (size_t)cap * d->capN), "alloc nj");
         CK(cudaMalloc((void **)&d->nd, sizeof(double) * 4 * (size_t)cap * d->capN), "alloc nd");
         if (p->legs_enabled && cap <= MB_LEG_MAX_CAP) {
@@ -406,6 +413,9 @@ static int ensure(mb_potential *p, int N, int nb, int ncell) {
             CK(cudaMalloc((void **)&d->nk, sizeof(unsigned) * (size_t)cap * d->capN), "alloc nk");
             CK(cudaMalloc((void **)&d->leg, sizeof(double) * MB_LEG_STRIDE * (size_t)cap * d->capN), "alloc legs");
             CK(cudaMalloc((void **)&d->nso, sizeof(int) * 4 * (size_t)d->capN), "alloc nso");
+            d->tcap = cap * (cap - 1) / 2;
+            CK(cudaMalloc((void **)&d->trip, sizeof(unsigned) * (size_t)d->tcap * d->capN), "alloc trip");
+            CK(cudaMalloc((void **)&d->tboff, sizeof(int) * 8 * (size_t)d->capN), "alloc tboff");
         }
         d->capNB = cap;
         p->gen++;

@@ -100,6 +100,9 @@ typedef struct {
 #define MB_MODE_EFS 2
 #define MB_MODE_VJP 3
 
+/* multi-CTA reductions (k_finalize, k_nvt_thermostat): at most this many CTAs */
+#define MB_RED_MAXB 64
+
 /* Device working set of one handle (all pointers are device memory). */
 typedef struct {
     int capN, capNB, capCells;
@@ -119,6 +122,8 @@ typedef struct {
     int *cell_start;  /* [capCells+1] */
     int *cell_atoms;  /* [N] */
     double *out;      /* [16] E, H, U[6], K, xi, ... */
+    double *part;     /* [2*MB_RED_MAXB*8] per-CTA partial sums of the reductions; NULL: one CTA */
+    unsigned *ticket; /* [2] CTAs finished, per reduction kernel (reset by the last one) */
     double *trace;    /* [2*steps] H and K per MD step */
     int capTrace;
     int *status;      /* [4]: flags, max neighbour count */
@@ -133,6 +138,12 @@ typedef struct {
     unsigned *nk;
     double *leg;
     int *nso;
+    /* triplet lists of the leg path (k_trip): trip[N*tcap] entries
+     * a | b << 8 | c << 16 per atom, tboff[8N] the species blocks' starts
+     * and the end; tcap = capNB (capNB - 1) / 2 bounds any atom's list */
+    unsigned *trip;
+    int *tboff;
+    int tcap;
     int legs_on;
     /* optional CUDA-event timing of the descriptor kernel */
     int ev_on, ev_n, ev_cap;

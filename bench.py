@@ -195,6 +195,13 @@ GEN_WORKLOAD = ("surrogate-screened EA generation: 4096 Cu-Pd-Ag offspring of 16
                 "20000 relaxed offspring; the best 25% by prediction are relaxed")
 
 
+def workloads_basis():
+    """The G2/G4 basis every workload's model uses (the reference bases' shape)."""
+    from maise_b200 import models
+
+    return models.Basis()
+
+
 def _binding_model(td, name, structures, spcz, seed, angular=0.3):
     from maise_b200 import models
 
@@ -237,6 +244,17 @@ def population_relax(local, td, plain_sample=64, mitr=1000, fmax=0.01, urep=100.
     batched = len(pop) / (rb["ms"] / 1e3)
     plain_sps = plain_sample / t_plain
     pot.close()
+    # FP32 roofline of k_relax_batch: the frozen counting rule over the pairs,
+    # forward triplets and atom evaluations the kernel counted, over its time
+    basis = workloads_basis()
+    flops = algorithmic_flops(basis, 2, rb["pairs"], rb["triplets"], rb["atom_evals"])
+    fp32 = maise_b200.fp32_peak_tflops(local)
+    ach = flops / (rb["ms"] * 1e-3) / 1e12
+    roof = {"bound": "fp32", "achieved": ach, "peak": fp32, "unit": "TFLOP/s", "frac": ach / fp32,
+            "kernel": "k_relax_batch (whole persistent launch: evaluations, BFGS, line search)",
+            "atom_evaluations": rb["atom_evals"], "pairs_per_atom_eval": rb["pairs"] / max(1, rb["atom_evals"]),
+            "triplets_per_atom_eval": rb["triplets"] / max(1, rb["atom_evals"]), "flops": flops,
+            "peak_source": "FP32 FMA-chain probe measured in this run"}
     return {"workload": POP_WORKLOAD, "structures": len(pop), "atoms": int(nat.sum()),
             "batched_structures_per_s": batched, "batched_e2e_structures_per_s": len(pop) / wall,
             "plain_structures_per_s": plain_sps, "speedup_vs_plain": batched / plain_sps,
@@ -244,7 +262,7 @@ def population_relax(local, td, plain_sample=64, mitr=1000, fmax=0.01, urep=100.
                             f"mb_relax_fmax each; their atom counts average {nat[sample].mean():.1f} against "
                             f"{nat.mean():.1f} for all",
             "batched_converged": int(conv.sum()), "plain_converged": int(sum(r["converged"] for r in plain)),
-            "batched_evals": rb["evals"], "kernel_ms": rb["ms"],
+            "batched_evals": rb["evals"], "kernel_ms": rb["ms"], "roofline": roof,
             "fp32_vs_fp64_ev_per_atom_max_converged": float(dE[conv].max()) if conv.any() else None,
             "fp64_max_force_converged_ev_per_a": float(f64[conv].max()) if conv.any() else None,
             "dtype": "descriptors/MLP fp32, reductions/BFGS fp64"}
@@ -344,6 +362,10 @@ def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs
             "recall_top10_random_expectation": keep,
             "generation_s_relax_all": t_all, "generation_s_screened": t_scr, "speedup": t_all / t_scr,
             "screen_s": t_pred, "relax_all_kernel_ms": ra["ms"], "relax_kept_kernel_ms": rk["ms"],
+            "work_kept_share": {"structures": len(kept) / n_gen,
+                                "atom_evaluations": rk["atom_evals"] / max(1, ra["atom_evals"]),
+                                "triplets": rk["triplets"] / max(1, ra["triplets"]),
+                                "kernel_time": rk["ms"] / max(1e-9, ra["ms"])},
             "train_data_relax_s": t_data, "fit_s": t_fit, "epochs": epochs, "final_loss": float(loss[-1]),
             "judge": "batched relax of every offspring (FP32 descriptors/MLP, FP64 BFGS)"}
 

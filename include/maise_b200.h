@@ -315,6 +315,15 @@ int mb_md_profile_read(mb_potential *pot, double *total_ms, int *steps);
  * mb_relax_batch call on this handle. */
 int mb_batch_stats(const mb_potential *pot, long long *evals, double *ms);
 
+/* Work of the last mb_relax_batch / mb_efs_batch launch: atom evaluations,
+ * neighbour pairs and forward triplets summed over all evaluations (the
+ * counts behind the batched kernel's FLOP rate). */
+int mb_batch_work(const mb_potential *pot, long long *atom_evals, long long *pairs, long long *triplets);
+
+/* Throughput of independent FP32 FMA chains filling every SM, TFLOP/s (the
+ * FP32 roofline denominator of the batched relax). */
+int mb_fp32_peak(int device, double *tflops);
+
 /* Sustained FP64 FMA throughput of `device` in TFLOP/s, measured with an
  * FMA-chain kernel over every SM (a roofline denominator for FP64 work). */
 int mb_fp64_peak(int device, double *tflops);

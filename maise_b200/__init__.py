@@ -85,6 +85,9 @@ def load_library():
     lib.mb_profile.argtypes = [vp, c_i, c_i]
     lib.mb_profile_read.argtypes = [vp, _D, _I, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
     lib.mb_fp64_peak.argtypes = [c_i, _D]
+    lib.mb_fp32_peak.argtypes = [c_i, _D]
+    lib.mb_batch_work.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                  ctypes.POINTER(ctypes.c_longlong)]
     lib.mb_md_profile.argtypes = [vp, c_i, c_i, ctypes.c_size_t]
     lib.mb_md_profile_read.argtypes = [vp, _D, _I]
     lib.CALL_MAISE.restype = c_d
@@ -124,6 +127,16 @@ def fp64_peak_tflops(device: int = 0) -> float:
     rc = lib.mb_fp64_peak(device, ctypes.byref(t))
     if rc:
         raise MaiseError(rc, "fp64 peak probe failed")
+    return t.value
+
+
+def fp32_peak_tflops(device: int = 0) -> float:
+    """Measured FP32 FMA throughput of the device (TFLOP/s)."""
+    lib = load_library()
+    t = ctypes.c_double()
+    rc = lib.mb_fp32_peak(device, ctypes.byref(t))
+    if rc:
+        raise MaiseError(rc, "fp32 peak probe failed")
     return t.value
 
 
@@ -361,9 +374,12 @@ class Potential:
                                             iters.ctypes.data_as(_I), status.ctypes.data_as(_I)))
         ev, ms = ctypes.c_longlong(), ctypes.c_double()
         self._check(self.lib.mb_batch_stats(self.h, ctypes.byref(ev), ctypes.byref(ms)))
+        wk = [ctypes.c_longlong() for _ in range(3)]
+        self._check(self.lib.mb_batch_work(self.h, *(ctypes.byref(v) for v in wk)))
         offs = np.concatenate([[0], np.cumsum(nat)])
         return dict(H=H, X=[X[offs[k]:offs[k + 1]] for k in range(S)], LAT=LAT, iters=iters, status=status,
-                    evals=int(ev.value), ms=float(ms.value))
+                    evals=int(ev.value), ms=float(ms.value), atom_evals=int(wk[0].value), pairs=int(wk[1].value),
+                    triplets=int(wk[2].value))
 
     def efs_batch(self, structures, p_gpa=0.0, urep=0.0):
         """FP32 batched E/F/S of a list of dict(X, LAT, atmn), no relaxation.

@@ -80,6 +80,9 @@ struct BArgs {
     float4 *nbd;   /* per CTA: BMAXN * BMAXNB */
     int *nbj;      /* per CTA: BMAXN * BMAXNB */
     long long *evals;
+    /* work done (for the roofline): atom evaluations, neighbour pairs and
+     * triplets of the forward pass; per-warp counts added at kernel exit */
+    unsigned long long *work;
 };
 
 struct WarpWS {
@@ -95,6 +98,7 @@ struct WarpWS {
     unsigned tl[BTL];
     int blk[6][2];
     int seg[8];
+    unsigned long long work[3]; /* atom evaluations, pairs, triplets of this warp */
 };
 
 template <int W>
@@ -282,6 +286,11 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
     const BParams &P = *A.P;
     const int lane = threadIdx.x & 31;
     const int n = sh.nn[i], s0 = sh.spc[i], ns = P.nspc, D = P.D, ng2 = P.ng2;
+    if (lane == 0) {
+        ws.work[0] += 1ull;
+        ws.work[1] += (unsigned long long)n;
+    }
+    int ntrip = 0; /* forward triplets this lane evaluated */
     /* stage neighbours stably sorted by relative species: counts and ranks
      * from warp ballots, one round per 32 neighbours */
     int cnt[4] = {0, 0, 0, 0};
@@ -433,6 +442,7 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
                     float dx = d1.x - d2.x, dy = d1.y - d2.y, dz = d1.z - d2.z;
                     float r3s = dx * dx + dy * dy + dz * dz, r3 = sqrtf(r3s);
                     if (!(d1.w < rc2_01 && d1.w < rc4_01 && d2.w < rc4_02 && r3s < rc4sq_12)) continue;
+                    ntrip++;
                     float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ws.ir[jj] * ws.ir[kk]);
                     float A3 = 2.0f * ws.fa[jj] * ws.fb[kk] * fcutf(rc4_12, r3);
                     float lz[BNZL];
@@ -566,6 +576,10 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
         }
     }
     __syncwarp();
+    {
+        const int t = __reduce_add_sync(FULLM, (unsigned)ntrip);
+        if (lane == 0) ws.work[2] += (unsigned long long)t;
+    }
 
     /* reverse triplets, reusing the lists when they fit */
     blkid = 0;
@@ -989,6 +1003,15 @@ __device__ void cluster_worker(const BArgs &A, BShared<W> &sh, int rank) {
     cl.sync();
 }
 
+/* each warp's work counts into the launch's totals (once per warp, at exit) */
+template <int W>
+__device__ void flush_work(const BArgs &A, BShared<W> &sh) {
+    if ((threadIdx.x & 31) == 0 && A.work) {
+        const WarpWS &ws = sh.ws[threadIdx.x >> 5];
+        for (int k = 0; k < 3; k++) atomicAdd(A.work + k, ws.work[k]);
+    }
+}
+
 /* cubic (or quadratic without db) minimiser on [lo,hi] (Fletcher, sec. 2.6) */
 __device__ double interp_min(double a, double fa, double da, double b, double fb, double db, double lo, double hi) {
     double w = b - a;
@@ -1031,10 +1054,14 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
     extern __shared__ __align__(16) char smem_raw[];
     BShared<W> &sh = *reinterpret_cast<BShared<W> *>(smem_raw);
     const int tid = threadIdx.x;
+    if ((tid & 31) == 0)
+        for (int k = 0; k < 3; k++) sh.ws[tid >> 5].work[k] = 0ull;
+    /* (every warp's first atom pass comes after a CTA or cluster barrier) */
     if constexpr (C > 1) {
         const int rank = (int)cooperative_groups::this_cluster().block_rank();
         if (rank != 0) {
             cluster_worker<W, C>(A, sh, rank);
+            flush_work(A, sh);
             return;
         }
     }
@@ -1266,6 +1293,7 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
         cooperative_groups::this_cluster().sync();
         cooperative_groups::this_cluster().sync();
     }
+    flush_work(A, sh);
 }
 
 }  // namespace
@@ -1368,6 +1396,7 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
                                const int *d_order, double *d_lat, double *d_x, double p_ev, double urep, int rlxt, int mitr, double fmax,
                                double *d_H, int *d_iters, int *d_status, double *d_frc, double *d_str,
                                void *stream, long long *evals_out, float *ms_out) {
+    /* evals_out[4]: evaluations, atom evaluations, pairs, triplets */
     cudaStream_t st = (cudaStream_t)stream;
     BParams hp;
     float *hw = nullptr;
@@ -1421,11 +1450,11 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
     if (!e) e = cudaMalloc(&nbd, sizeof(float4) * (size_t)grid * BMAXN * BMAXNB);
     if (!e) e = cudaMalloc(&nbj, sizeof(int) * (size_t)grid * BMAXN * BMAXNB);
     if (!e) e = cudaMalloc(&queue, sizeof(int));
-    if (!e) e = cudaMalloc(&evals, sizeof(long long));
+    if (!e) e = cudaMalloc(&evals, 4 * sizeof(long long));
     if (!e) e = cudaMemcpyAsync(dp, &hp, sizeof(BParams), cudaMemcpyHostToDevice, st);
     if (!e) e = cudaMemcpyAsync(dw, hw, sizeof(float) * wlen, cudaMemcpyHostToDevice, st);
     if (!e) e = cudaMemsetAsync(queue, 0, sizeof(int), st);
-    if (!e) e = cudaMemsetAsync(evals, 0, sizeof(long long), st);
+    if (!e) e = cudaMemsetAsync(evals, 0, 4 * sizeof(long long), st);
     if (!e) {
         BArgs a;
         a.S = S; a.rlxt = rlxt; a.mitr = mitr;
@@ -1434,6 +1463,7 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
         a.lat = d_lat; a.x = d_x; a.H = d_H; a.iters = d_iters; a.status = d_status;
         a.fout = d_frc; a.uout = d_str;
         a.P = dp; a.W = dw; a.queue = queue; a.hmat = hm; a.nbd = nbd; a.nbj = nbj; a.evals = evals;
+        a.work = (unsigned long long *)(evals + 1);
         cudaEventRecord(e0, st);
         e = !wide        ? batch_launch<4, 1>(gunits, st, a)
             : csize == 4 ? batch_launch<BWARPS_WIDE, 4>(gunits, st, a)
@@ -1443,7 +1473,7 @@ extern "C" int mbk_relax_batch(const mb_model *m, int S, const int *d_nat, const
         if (!e) e = cudaGetLastError();
     }
     if (!e) e = cudaStreamSynchronize(st);
-    if (!e && evals_out) e = cudaMemcpy(evals_out, evals, sizeof(long long), cudaMemcpyDeviceToHost);
+    if (!e && evals_out) e = cudaMemcpy(evals_out, evals, 4 * sizeof(long long), cudaMemcpyDeviceToHost);
     if (!e && ms_out) cudaEventElapsedTime(ms_out, e0, e1);
     cudaFree(dp); cudaFree(dw); cudaFree(hm); cudaFree(nbd); cudaFree(nbj); cudaFree(queue); cudaFree(evals);
     cudaEventDestroy(e0);

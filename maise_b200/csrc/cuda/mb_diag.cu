@@ -1,7 +1,8 @@
 /*
- * mb_diag.cu -- FP64 FMA throughput probe.  Each thread runs independent
- * FMA chains; the kernel fills every SM with resident warps.  The measured
- * rate is the denominator of the FP64 roofline of the descriptor kernel.
+ * mb_diag.cu -- FMA throughput probes (FP64 and FP32).  Each thread runs
+ * independent FMA chains; the kernel fills every SM with resident warps.
+ * The measured rates are the denominators of the FP64 roofline of the
+ * descriptor kernels and the FP32 roofline of the batched relax.
  */
 #include <cuda_runtime.h>
 
@@ -11,39 +12,43 @@ namespace {
 
 constexpr int CHAINS = 8;
 
-__global__ void k_fma_chains(double *out, int iters, double a, double b) {
-    double v[CHAINS];
+template <class T>
+__global__ void k_fma_chains(T *out, int iters, T a, T b) {
+    T v[CHAINS];
 #pragma unroll
-    for (int c = 0; c < CHAINS; c++) v[c] = threadIdx.x * 1e-9 + c;
+    for (int c = 0; c < CHAINS; c++) v[c] = (T)(threadIdx.x * 1e-9 + c);
     for (int it = 0; it < iters; it++) {
 #pragma unroll
         for (int c = 0; c < CHAINS; c++) v[c] = fma(v[c], a, b);
     }
-    double s = 0.0;
+    T s = 0;
 #pragma unroll
     for (int c = 0; c < CHAINS; c++) s += v[c];
-    if (s == 12345.678) out[0] = s; /* keeps the chains live */
+    if (s == (T)12345.678) out[0] = s; /* keeps the chains live */
 }
 
 }  // namespace
 
-extern "C" int mb_fp64_peak(int device, double *tflops) {
+template <class T>
+static int fma_peak(int device, double *tflops) {
     cudaDeviceProp prop;
-    double *out = nullptr;
+    T *out = nullptr;
     cudaEvent_t e0, e1;
     const int threads = 256, iters = 4096;
+    if (!tflops) return MB_ERR_ARG;
     if (cudaSetDevice(device) != cudaSuccess || cudaGetDeviceProperties(&prop, device) != cudaSuccess)
         return MB_ERR_NOGPU;
     int blocks = prop.multiProcessorCount * 8;
-    if (cudaMalloc(&out, sizeof(double)) != cudaSuccess) return MB_ERR_CUDA;
+    if (cudaMalloc(&out, sizeof(T)) != cudaSuccess) return MB_ERR_CUDA;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    k_fma_chains<<<blocks, threads>>>(out, iters, 0.999999, 1e-7); /* warm-up */
+    const T a = (T)0.999999, b = (T)1e-7;
+    k_fma_chains<T><<<blocks, threads>>>(out, iters, a, b); /* warm-up */
     float best = 1e30f;
     for (int rep = 0; rep < 5; rep++) {
         float ms = 0.0f;
         cudaEventRecord(e0);
-        k_fma_chains<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+        k_fma_chains<T><<<blocks, threads>>>(out, iters, a, b);
         cudaEventRecord(e1);
         cudaEventSynchronize(e1);
         cudaEventElapsedTime(&ms, e0, e1);
@@ -58,3 +63,7 @@ extern "C" int mb_fp64_peak(int device, double *tflops) {
     *tflops = flops / (best * 1e-3) / 1e12;
     return MB_OK;
 }
+
+extern "C" int mb_fp64_peak(int device, double *tflops) { return fma_peak<double>(device, tflops); }
+
+extern "C" int mb_fp32_peak(int device, double *tflops) { return fma_peak<float>(device, tflops); }

@@ -154,29 +154,37 @@ __global__ void k_cell_bin(int N, const double *__restrict__ X, mb_cell c, int *
     atomicAdd(&cnt[k], 1);
 }
 
-/* exclusive scan of the cell counts by one CTA; start[ncell] = N */
+/* exclusive scan of the cell counts by one CTA of 1024 threads; start[ncell] = N */
 __global__ void k_cell_scan(int ncell, const int *cnt, int *start) {
-    __shared__ int part[1024];
-    int t = threadIdx.x, nt = blockDim.x;
-    int per = (ncell + nt - 1) / nt, lo = t * per, hi = min(lo + per, ncell), s = 0;
+    __shared__ int wsum[32];
+    const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, w = t >> 5;
+    const int per = (ncell + nt - 1) / nt, lo = t * per, hi = min(lo + per, ncell);
+    int s = 0;
     for (int k = lo; k < hi; k++) s += cnt[k];
-    part[t] = s;
+    int x = s; /* inclusive scan over the warp */
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
     __syncthreads();
-    if (t == 0) {
-        int acc = 0;
-        for (int k = 0; k < nt; k++) {
-            int v = part[k];
-            part[k] = acc;
-            acc += v;
+    if (w == 0) {
+        int v = lane < (nt >> 5) ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, v, o);
+            if (lane >= o) v += y;
         }
+        wsum[lane] = v;
     }
     __syncthreads();
-    s = part[t];
+    int e = x - s + (w > 0 ? wsum[w - 1] : 0);
     for (int k = lo; k < hi; k++) {
-        start[k] = s;
-        s += cnt[k];
+        start[k] = e;
+        e += cnt[k];
     }
-    if (t == nt - 1) start[ncell] = s;
+    if (t == nt - 1) start[ncell] = e;
 }
 
 __global__ void k_cell_fill(int N, const int *cell_of, const int *start, int *cursor, int *atoms) {
@@ -1278,7 +1286,7 @@ struct LegArgs {
     const int *nn, *nj, *nso;
     const double4 *nd;
     const double *leg;
-    const unsigned *trip; /* triplet lists (k_trip) */
+    const uint2 *trip; /* triplet lists (k_trip) */
     const int *tboff;
     int tcap;
     const int *spc;
@@ -1287,6 +1295,7 @@ struct LegArgs {
     double *EA, *EU, *G, *F, *vir;
     unsigned long long *counters;
     size_t smem_group;
+    mb_params P; /* by value: read from the kernel-parameter space through the constant cache */
 };
 
 /* shared-memory carve-up of one atom group of k_efs_leg */
@@ -1333,9 +1342,6 @@ __device__ inline LegSmem leg_carve(char *base, int cap, int D, int ng2, int war
 
 __device__ __forceinline__ unsigned hash_slot(unsigned key) { return (key * 0x9E3779B1u) >> 24; }
 
-/* start of species s in a list whose species starts are o (nso layout) */
-__device__ __forceinline__ int jo_at(const int4 &o, int s) { return s == 0 ? o.x : (s == 1 ? o.y : (s == 2 ? o.z : o.w)); }
-
 /* Triplet lists of the leg path: one warp per atom i, TRIP_WARPS atoms per
  * CTA.  The warp stages i's entries in relative-species order (position u,
  * the order k_efs_leg stages them in: relative species v holds absolute
@@ -1348,29 +1354,45 @@ __device__ __forceinline__ int jo_at(const int4 &o, int s) { return s == 0 ? o.x
  * slot b > a makes (a, b) a triplet with r_ij, r_ik and r_jk below Rc
  * (each (k, image) of j's list is a distinct image relative to i, so a
  * pair (a, b) is found at most once and a list never exceeds
- * tcap = cap (cap - 1) / 2).  Accepted entries a | b << 8 | c << 16 are
- * written in candidate order (a ascending, then c), so every list is
+ * tcap = cap (cap - 1) / 2).  Accepted entries {a | b << 8, row} -- row =
+ * j cap + c, the j-k leg row -- are written in candidate order (a
+ * ascending, then c), so every list is
  * deterministic; tboff[8 i + blk] holds the start of each block and
  * tboff[8 i + nblk] the end.  counters[1] (if set) receives the number of
  * triplets. */
 #define TRIP_WARPS 8
+
+/* The 15-bit image field of an entry key (three 5-bit two's-complement
+ * shifts) spread into 7-bit fields with the bias +16, so that the image of
+ * a sum of two displacements is one integer add: field t = x_a + x_c + 48,
+ * in [32, 63] exactly when the summed shift lies in [-16, 15]. */
+__device__ __forceinline__ unsigned spread_img(unsigned key) {
+    const unsigned f = (key & 0x7fffu) ^ 0x4210u; /* x + 16 per field */
+    return (f & 31u) | ((f & (31u << 5)) << 2) | ((f & (31u << 10)) << 4);
+}
+#define IMG_BIAS (16u | (16u << 7) | (16u << 14))
+#define IMG_BIT5 ((1u << 5) | (1u << 12) | (1u << 19))
+#define IMG_BIT6 ((1u << 6) | (1u << 13) | (1u << 20))
+
 __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tcap, int ns, const int *__restrict__ nn,
                                                           const int *__restrict__ nj, const unsigned *__restrict__ nk,
                                                           const int *__restrict__ nso, const int *__restrict__ spc,
-                                                          unsigned *__restrict__ trip, int *__restrict__ tboff,
+                                                          uint2 *__restrict__ trip, int *__restrict__ tboff,
                                                           unsigned long long *counters) {
     __shared__ uint2 hsh[TRIP_WARPS][LEG_HASH];
-    __shared__ int sj[TRIP_WARPS][MB_LEG_MAX_CAP];
-    __shared__ unsigned skey[TRIP_WARPS][MB_LEG_MAX_CAP];
-    __shared__ int4 sjo[TRIP_WARPS][MB_LEG_MAX_CAP];
+    /* per staged entry a: its atom j, j cap (j's list row), the spread image
+     * of its key plus the bias, and (per species block) where j's entries of
+     * the block's second species start and how many there are */
+    __shared__ int sj[TRIP_WARPS][MB_LEG_MAX_CAP], srow[TRIP_WARPS][MB_LEG_MAX_CAP];
+    __shared__ unsigned simg[TRIP_WARPS][MB_LEG_MAX_CAP];
+    __shared__ int sst[TRIP_WARPS][MB_LEG_MAX_CAP], slen[TRIP_WARPS][MB_LEG_MAX_CAP];
     __shared__ int sseg[TRIP_WARPS][8];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * TRIP_WARPS + w;
     if (i >= N) return; /* whole warps; nothing below synchronises the CTA */
     uint2 *hash = hsh[w];
-    int *js = sj[w], *seg = sseg[w];
-    unsigned *key = skey[w];
-    int4 *jo = sjo[w];
+    int *js = sj[w], *rowj = srow[w], *st = sst[w], *len = slen[w], *seg = sseg[w];
+    unsigned *img = simg[w];
     const int n = nn[i], s0 = spc[i];
     const size_t row = (size_t)i * cap;
     if (lane < 4) {
@@ -1392,13 +1414,10 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
         const int sa = (s0 + v) % ns;
         const int t = nso[4 * i + sa] + (u - seg[4 + v]);
         const int j = nj[row + t];
+        const unsigned k = nk[row + t];
         js[u] = j;
-        key[u] = nk[row + t];
-        jo[u] = *reinterpret_cast<const int4 *>(nso + 4 * (size_t)j);
-    }
-    __syncwarp();
-    for (int u = lane; u < n; u += 32) {
-        const unsigned k = key[u];
+        rowj[u] = j * cap;
+        img[u] = spread_img(k) + IMG_BIAS;
         unsigned h = hash_slot(k);
         for (int probe = 0; probe < LEG_HASH; probe++) {
             if (atomicCAS(&hash[h].x, 0xffffffffu, k) == 0xffffffffu) {
@@ -1409,37 +1428,37 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
         }
     }
     __syncwarp();
-    unsigned *out = trip + (size_t)i * tcap;
+    uint2 *out = trip + (size_t)i * tcap;
     int pos = 0, blkid = 0;
     for (int al = 0; al < ns; al++)
         for (int be = al; be < ns; be++, blkid++) {
             if (lane == 0) tboff[8 * i + blkid] = pos;
-            const int sb = (s0 + be) % ns, a_hi = seg[4 + al] + seg[al];
-            int ca = seg[4 + al], cc = lane;
-            /* the lane's candidate (ca, cc): entry cc of species sb in the list of i's entry ca */
-            auto norm = [&]() {
-                while (ca < a_hi) {
-                    const int4 o = jo[ca];
-                    const int len = jo_at(o, sb + 1) - jo_at(o, sb);
-                    if (cc < len) break;
-                    cc -= len;
-                    ca++;
-                }
-            };
-            norm();
+            const int sb = (s0 + be) % ns, a_lo = seg[4 + al], a_hi = a_lo + seg[al];
+            for (int a = a_lo + lane; a < a_hi; a += 32) {
+                const int *o = nso + 4 * (size_t)js[a];
+                st[a] = o[sb];
+                len[a] = o[sb + 1] - o[sb];
+            }
+            __syncwarp();
+            /* the lane's candidate (ca, cc): entry cc of j's species-sb entries, j = atom of i's entry ca */
+            int ca = a_lo, cc = lane;
+            while (ca < a_hi && cc >= len[ca]) {
+                cc -= len[ca];
+                ca++;
+            }
             for (;;) {
                 const bool live = ca < a_hi;
                 if (!__any_sync(FULL, live)) break;
                 bool ok = false;
-                unsigned ent = 0u;
+                uint2 ent = make_uint2(0u, 0u);
                 if (live) {
-                    const int c = jo_at(jo[ca], sb) + cc;
-                    const unsigned kc = __ldg(nk + (size_t)js[ca] * cap + c), ka = key[ca];
-                    const int x0 = sx5(ka >> 10) + sx5(kc >> 10), x1 = sx5(ka >> 5) + sx5(kc >> 5),
-                              x2 = sx5(ka) + sx5(kc);
-                    if (x0 >= -16 && x0 <= 15 && x1 >= -16 && x1 <= 15 && x2 >= -16 && x2 <= 15) {
-                        const unsigned kk = (kc & ~0x7fffu) | (((unsigned)x0 & 31u) << 10) |
-                                            (((unsigned)x1 & 31u) << 5) | ((unsigned)x2 & 31u);
+                    const unsigned r = (unsigned)(rowj[ca] + st[ca] + cc);
+                    const unsigned kc = __ldg(nk + r);
+                    const unsigned t = spread_img(kc) + img[ca];
+                    if ((t & IMG_BIT6) == 0u && (t & IMG_BIT5) == IMG_BIT5) {
+                        /* back to three 5-bit two's-complement fields */
+                        const unsigned f = (t & 31u) | ((t >> 2) & (31u << 5)) | ((t >> 4) & (31u << 10));
+                        const unsigned kk = (kc & ~0x7fffu) | (f ^ 0x4210u);
                         unsigned h = hash_slot(kk);
                         int b = -1;
                         for (int probe = 0; probe < LEG_HASH; probe++) {
@@ -1452,15 +1471,19 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
                             h = (h + 1u) & (LEG_HASH - 1u);
                         }
                         ok = b > ca;
-                        ent = (unsigned)ca | ((unsigned)b << 8) | ((unsigned)c << 16);
+                        ent = make_uint2((unsigned)ca | ((unsigned)b << 8), r);
                     }
                 }
                 const unsigned m = __ballot_sync(FULL, ok);
                 if (ok) out[pos + __popc(m & ((1u << lane) - 1u))] = ent;
                 pos += __popc(m);
                 cc += 32;
-                norm();
+                while (ca < a_hi && cc >= len[ca]) {
+                    cc -= len[ca];
+                    ca++;
+                }
             }
+            __syncwarp();
         }
     if (lane == 0) {
         tboff[8 * i + blkid] = pos;
@@ -1473,18 +1496,18 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
  * consecutive entries mostly share a, so the a-side forces are summed in
  * registers and added to Fnb once per change of a. */
 template <class Body>
-__device__ __forceinline__ void leg_run_runs(const LegSmem &s, const unsigned *__restrict__ list, int from, int to,
+__device__ __forceinline__ void leg_run_runs(const LegSmem &s, const uint2 *__restrict__ list, int from, int to,
                                              int lane, Body body) {
     int K = (to - from + 31) >> 5;
     if (K > 0) K |= 1;
-    const int t0 = from + lane * K;
+    const int t0 = from + lane * K, t1 = min(to, t0 + K);
     int ca = -1;
     double sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int step = 0; step < K; step++) {
-        const int t = t0 + step;
-        if (t >= to) break;
-        const unsigned ent = __ldg(list + t);
-        const int a = (int)(ent & 0xffu);
+    uint2 nxt = t0 < t1 ? __ldg(list + t0) : make_uint2(0u, 0u);
+    for (int t = t0; t < t1; t++) {
+        const uint2 ent = nxt;
+        if (t + 1 < t1) nxt = __ldg(list + t + 1); /* the next entry is in flight while this one is computed */
+        const int a = (int)(ent.x & 0xffu);
         if (a != ca) {
             if (ca >= 0) {
                 atomicAdd(&s.Fnb[3 * ca], -sx);
@@ -1511,26 +1534,28 @@ __device__ __forceinline__ void leg_run_runs(const LegSmem &s, const unsigned *_
  * read from the rows k_legs wrote (i-j and i-k from i's own rows, staged;
  * j-k from j's row in global memory, L2-resident).  Reference bases: at
  * most 8 G4 exponents, zeta in {1, 2, 4, 16} or other integers, 2 lambdas. */
+/* every shape is compiled for 12 resident warps per SM (at most 170
+ * registers a thread), the occupancy its shared memory also allows at the
+ * alloy's neighbour counts */
 template <int NE, int WPA, int APB>
-__global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
+__global__ void __launch_bounds__(WPA * 32 * APB, 384 / (WPA * 32 * APB)) k_efs_leg(const __grid_constant__ LegArgs A) {
     constexpr int NZ = 4, NLAM = 2, NZL = 8;
     static_assert(NE == 7 || NE == 8, "leg rows hold 8 exponents");
     extern __shared__ __align__(16) char smem_raw[];
-    __shared__ mb_params Ps;
-    {
-        const int *src = reinterpret_cast<const int *>(A.params);
-        int *dst = reinterpret_cast<int *>(&Ps);
-        for (int k = threadIdx.x; k < (int)(sizeof(mb_params) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
-        __syncthreads();
-    }
-    const mb_params &P = Ps;
+    const mb_params &P = A.P;
+    /* G4 feature -> cell of the (eta, zeta-lambda) grid: the one table read
+     * at a different index by every thread, so it is kept in shared memory */
+    __shared__ unsigned char g4cell[MB_MAXG4];
+    for (int f = threadIdx.x; f < P.ng4; f += blockDim.x)
+        g4cell[f] = (unsigned char)(P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam);
+    __syncthreads();
     const int NT = WPA * 32, group = threadIdx.x / NT;
     const int tid = threadIdx.x % NT, lane = threadIdx.x & 31, warp = tid >> 5;
     const int i = blockIdx.x * APB + group;
     if (i >= A.N) return; /* whole atom groups only: no barrier spans two groups */
     const int D = P.D, ns = P.nspc, ng2 = P.ng2, ne = P.ne, cap = A.cap;
     LegSmem s = leg_carve(smem_raw + (size_t)group * A.smem_group, cap, D, ng2, WPA);
-    const unsigned *tl = A.trip + (size_t)i * A.tcap;
+    const uint2 *tl = A.trip + (size_t)i * A.tcap;
     const int *tb = A.tboff + 8 * (size_t)i;
     const int n = A.nn[i];
     const int s0 = A.spc[i];
@@ -1605,20 +1630,19 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
             for (int be = al; be < ns; be++, blkid++) {
                 double c0 = 0.0, c1 = 0.0;
                 double *stw = s.stage + warp * 32 * EFS_STG;
-                auto body = [&](unsigned ent, bool valid) {
+                auto body = [&](uint2 ent, bool valid) {
                     double ex[8], lz[NZL];
 #pragma unroll
                     for (int q = 0; q < 8; q++) ex[q] = 0.0;
 #pragma unroll
                     for (int q = 0; q < NZL; q++) lz[q] = 0.0;
                     if (valid) {
-                        const int a = (int)(ent & 0xffu), b = (int)((ent >> 8) & 0xffu), cj = (int)(ent >> 16);
+                        const int a = (int)(ent.x & 0xffu), b = (int)((ent.x >> 8) & 0xffu);
                         const double4 d1 = s.d[a], d2 = s.d[b];
                         const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (s.ir[a] * s.ir[b]);
                         const double2 *la = reinterpret_cast<const double2 *>(s.L + a * MB_LEG_STRIDE);
                         const double2 *lb = reinterpret_cast<const double2 *>(s.L + b * MB_LEG_STRIDE);
-                        const double2 *lg =
-                            reinterpret_cast<const double2 *>(A.leg + ((size_t)s.j[a] * cap + cj) * MB_LEG_STRIDE);
+                        const double2 *lg = reinterpret_cast<const double2 *>(A.leg + (size_t)ent.y * MB_LEG_STRIDE);
                         const double A3 = 2.0 * la[4].x * lb[4].x * __ldg(lg + 4).x;
                         angular<NZ, NLAM>(P, c, lz, nullptr);
 #pragma unroll
@@ -1643,16 +1667,23 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
                     __syncwarp();
                 };
                 /* the block's list entries, 32 per round, the atom's warps taking every WPA-th round */
-                for (int base = tb[blkid] + warp * 32, to = tb[blkid + 1]; base < to; base += 32 * WPA) {
-                    const int t = base + lane;
-                    body(t < to ? __ldg(tl + t) : 0u, t < to);
+                {
+                    const int to = tb[blkid + 1];
+                    int base = tb[blkid] + warp * 32;
+                    uint2 cur = base + lane < to ? __ldg(tl + base + lane) : make_uint2(0u, 0u);
+                    for (; base < to; base += 32 * WPA) {
+                        /* the next round's entry is in flight while this round is computed */
+                        const int tn = base + 32 * WPA + lane;
+                        const uint2 nxt = tn < to ? __ldg(tl + tn) : make_uint2(0u, 0u);
+                        body(cur, base + lane < to);
+                        cur = nxt;
+                    }
                 }
                 group_sync<WPA>();
                 group_store64<WPA>(c0, c1, s, warp, lane);
                 {
                     const int base = P.ind4[al * al + be * be];
-                    for (int f = tid; f < P.ng4; f += NT)
-                        s.G[base + f] += s.red[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam];
+                    for (int f = tid; f < P.ng4; f += NT) s.G[base + f] += s.red[g4cell[f]];
                 }
                 group_sync<WPA>();
             }
@@ -1752,18 +1783,17 @@ __global__ void __launch_bounds__(WPA * 32 * APB) k_efs_leg(LegArgs A) {
                 for (int t = tid; t < 64; t += NT) s.grid[t] = 0.0;
                 group_sync<WPA>();
                 for (int f = tid; f < P.ng4; f += NT)
-                    atomicAdd(&s.grid[P.g4_e[f] * NZL + (P.g4_zl[f] / P.nlam) * NLAM + P.g4_zl[f] % P.nlam], s.G[base + f]);
+                    atomicAdd(&s.grid[g4cell[f]], s.G[base + f]);
                 group_sync<WPA>();
-                auto body = [&](unsigned ent) -> double3 {
-                    const int a = (int)(ent & 0xffu), b = (int)((ent >> 8) & 0xffu), cj = (int)(ent >> 16);
+                auto body = [&](uint2 ent) -> double3 {
+                    const int a = (int)(ent.x & 0xffu), b = (int)((ent.x >> 8) & 0xffu);
                     const double4 d1 = s.d[a], d2 = s.d[b];
                     const double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
                     const double ir1 = s.ir[a], ir2 = s.ir[b];
                     const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
                     const double2 *la = reinterpret_cast<const double2 *>(s.L + a * MB_LEG_STRIDE);
                     const double2 *lb = reinterpret_cast<const double2 *>(s.L + b * MB_LEG_STRIDE);
-                    const double2 *lg =
-                        reinterpret_cast<const double2 *>(A.leg + ((size_t)s.j[a] * cap + cj) * MB_LEG_STRIDE);
+                    const double2 *lg = reinterpret_cast<const double2 *>(A.leg + (size_t)ent.y * MB_LEG_STRIDE);
                     const double2 fa = la[4], fb = lb[4], fg = __ldg(lg + 4);
                     double lz[NZL], lzp[NZL];
 #pragma unroll
@@ -2122,6 +2152,7 @@ struct EfsShape {
 };
 static const EfsShape kShapes[] = {{1, 4}, {4, 1}, {8, 1}};
 #define EFS_STATIC_SMEM (sizeof(mb_params) + 16) /* k_efs's __shared__ Ps, with alignment slack */
+#define LEG_STATIC_SMEM (MB_MAXG4 + 16)          /* k_efs_leg's __shared__ g4cell */
 #define MB_NSHAPES 3
 #define MB_MAX_DEVICES_K 64
 
@@ -2274,8 +2305,8 @@ static int launch_leg(const LegArgs &a, cudaStream_t st) {
     static size_t configured[MB_MAX_DEVICES_K] = {0};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MB_MAX_DEVICES_K) return (int)cudaErrorInvalidDevice;
-    if (smem + EFS_STATIC_SMEM > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
-    if (smem + EFS_STATIC_SMEM > 48 * 1024 && smem > configured[dev]) {
+    if (smem + LEG_STATIC_SMEM > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
+    if (smem + LEG_STATIC_SMEM > 48 * 1024 && smem > configured[dev]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
         configured[dev] = smem;
@@ -2292,7 +2323,7 @@ static int launch_leg_pass(const mb_dev *d, const mb_model *m, int shape, LegArg
     k_legs<<<(a.N + 3) / 4, 128, 0, st>>>(a.N, a.cap, d->nn, d->nj, d->nk, (double4 *)d->nd, d->spc, d->params,
                                          d->leg, d->nso);
     k_trip<<<(a.N + TRIP_WARPS - 1) / TRIP_WARPS, 32 * TRIP_WARPS, 0, st>>>(
-        a.N, a.cap, d->tcap, m->P.nspc, d->nn, d->nj, d->nk, d->nso, d->spc, d->trip, d->tboff, a.counters);
+        a.N, a.cap, d->tcap, m->P.nspc, d->nn, d->nj, d->nk, d->nso, d->spc, (uint2 *)d->trip, d->tboff, a.counters);
     int rc;
     if (m->P.ne <= 7) {
         switch (shape) {
@@ -2353,7 +2384,7 @@ static int tune_leg(mb_dev *d, const mb_model *m, int N, int mode, const LegArgs
     int best = 0;
     float best_ms = 1e30f;
     for (int sh = 0; sh < MB_NLEGSHAPES; sh++) {
-        if (leg_group_bytes(m, a.cap, kLegShapes[sh].wpa) * kLegShapes[sh].apb + EFS_STATIC_SMEM > 227 * 1024) continue;
+        if (leg_group_bytes(m, a.cap, kLegShapes[sh].wpa) * kLegShapes[sh].apb + LEG_STATIC_SMEM > 227 * 1024) continue;
         float ms = 1e30f;
         int bad = 0;
         for (int rep = 0; rep < 2 && !bad; rep++) {
@@ -2455,7 +2486,7 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
         la.nj = d->nj;
         la.nso = d->nso;
         la.nd = (const double4 *)d->nd;
-        la.trip = d->trip;
+        la.trip = (const uint2 *)d->trip;
         la.tboff = d->tboff;
         la.tcap = d->tcap;
         la.leg = d->leg;
@@ -2469,6 +2500,7 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
         la.vir = d->vir;
         la.counters = d->counters;
         la.smem_group = 0;
+        la.P = m->P;
         const int shape = tune_leg(d, m, N, mode, la, st);
         d->last_shape = 16 + shape;
         cudaEvent_t e0 = 0, e1 = 0;

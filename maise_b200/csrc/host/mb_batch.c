@@ -18,7 +18,7 @@ const mb_model *mb_handle_model(const mb_potential *p);
 void *mb_handle_stream(mb_potential *p);
 int mb_handle_device(const mb_potential *p);
 int mb_handle_fail(int code, const char *msg);
-void mb_handle_set_batch_stats(mb_potential *p, long long evals, float ms);
+void mb_handle_set_batch_stats(mb_potential *p, const long long *evals, float ms);
 
 /* The population relax and the batched E/F/S share this: with frc/str set
  * the kernel also returns each structure's forces and virial at its final
@@ -29,7 +29,7 @@ static int batch_run(mb_potential *pot, int S, const int *nat, const int *atmn, 
     int *off, *order, total = 0, s, rc = MB_OK;
     int *d_nat = NULL, *d_off = NULL, *d_spc = NULL, *d_iters = NULL, *d_status = NULL, *d_order = NULL;
     double *d_lat = NULL, *d_x = NULL, *d_H = NULL, *d_frc = NULL, *d_str = NULL;
-    long long evals = 0;
+    long long evals[4] = {0, 0, 0, 0}; /* evaluations, atom evaluations, pairs, triplets */
     float ms = 0.0f;
     const mb_model *m;
     void *st;
@@ -87,7 +87,7 @@ static int batch_run(mb_potential *pot, int S, const int *nat, const int *atmn, 
     }
     e = (cudaError_t)mbk_relax_batch(m, S, d_nat, d_off, d_spc, d_order, d_lat, d_x, p_gpa / MB_EV2GPA, urep > 0 ? urep : 0.0,
                                      rlxt, mitr, fmax, d_H, d_iters, d_status, frc ? d_frc : NULL,
-                                     frc ? d_str : NULL, st, &evals, &ms);
+                                     frc ? d_str : NULL, st, evals, &ms);
     if (e == cudaErrorInvalidValue) {
         rc = mb_handle_fail(MB_ERR_MODEL, "batched relax needs a basis with <= 7 G4 exponents, zeta in {integers}, "
                                           "2 lambdas, <= 16 G2 functions and D <= 288");

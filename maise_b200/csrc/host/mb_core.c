@@ -59,7 +59,7 @@ typedef struct {
 struct mb_potential {
     mb_model m;
     int device;
-    long long batch_evals;
+    long long batch_evals, batch_work[3];
     float batch_ms;
     cudaStream_t stream;
     mb_dev d;
@@ -241,8 +241,11 @@ const mb_model *mb_handle_model(const mb_potential *p) { return &p->m; }
 void *mb_handle_stream(mb_potential *p) { return (void *)p->stream; }
 int mb_handle_device(const mb_potential *p) { return p->device; }
 int mb_handle_fail(int code, const char *msg) { return fail(code, "%s", msg); }
-void mb_handle_set_batch_stats(mb_potential *p, long long evals, float ms) {
-    p->batch_evals = evals;
+void mb_handle_set_batch_stats(mb_potential *p, const long long *evals, float ms) {
+    p->batch_evals = evals[0];
+    p->batch_work[0] = evals[1];
+    p->batch_work[1] = evals[2];
+    p->batch_work[2] = evals[3];
     p->batch_ms = ms;
 }
 
@@ -267,6 +270,14 @@ int mb_tune_read(const mb_potential *p, int cap, int *count, int *mode, int *leg
         capacity[k] = key & 0xfffff;
         if (mbk_shape_dims(lg, p->d.tune_val[k], &wpa[k], &apb[k])) wpa[k] = apb[k] = 0;
     }
+    return MB_OK;
+}
+
+int mb_batch_work(const mb_potential *p, long long *atom_evals, long long *pairs, long long *triplets) {
+    if (!p) return fail(MB_ERR_ARG, "null handle");
+    if (atom_evals) *atom_evals = p->batch_work[0];
+    if (pairs) *pairs = p->batch_work[1];
+    if (triplets) *triplets = p->batch_work[2];
     return MB_OK;
 }
 
@@ -414,7 +425,7 @@ static int ensure(mb_potential *p, int N, int nb, int ncell) {
             CK(cudaMalloc((void **)&d->leg, sizeof(double) * MB_LEG_STRIDE * (size_t)cap * d->capN), "alloc legs");
             CK(cudaMalloc((void **)&d->nso, sizeof(int) * 4 * (size_t)d->capN), "alloc nso");
             d->tcap = cap * (cap - 1) / 2;
-            CK(cudaMalloc((void **)&d->trip, sizeof(unsigned) * (size_t)d->tcap * d->capN), "alloc trip");
+            CK(cudaMalloc((void **)&d->trip, 2 * sizeof(unsigned) * (size_t)d->tcap * d->capN), "alloc trip");
             CK(cudaMalloc((void **)&d->tboff, sizeof(int) * 8 * (size_t)d->capN), "alloc tboff");
         }
         d->capNB = cap;

@@ -139,9 +139,9 @@ typedef struct {
     double *leg;
     int *nso;
     /* triplet lists of the leg path (k_trip): trip[N*tcap] entries
-     * a | b << 8 | c << 16 per atom, tboff[8N] the species blocks' starts
-     * and the end; tcap = capNB (capNB - 1) / 2 bounds any atom's list */
-    unsigned *trip;
+     * {a | b << 8, j-k leg row} per atom, tboff[8N] the species blocks'
+     * starts and the end; tcap = capNB (capNB - 1) / 2 bounds any list */
+    void *trip;
     int *tboff;
     int tcap;
     int legs_on;

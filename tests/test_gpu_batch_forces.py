@@ -75,3 +75,25 @@ def test_batched_efs_matches_relax_batch_enthalpy(population):
     b = pot.relax_batch(sub, urep=UREP, rlxt=3, mitr=0, fmax=0.01)
     nat = np.array([len(s["atmn"]) for s in sub])
     np.testing.assert_allclose(a["H"] / nat, b["H"] / nat, atol=1e-6)
+
+
+def test_batched_work_counts_match_the_plain_path(population):
+    """The pair and triplet counts k_relax_batch reports for its FP32 roofline
+    (mb_batch_work) are the plain path's: every evaluation of a structure
+    sees its LIST neighbour pairs and the triplets with all three legs
+    inside Rc, as the descriptor pass counts them."""
+    pot, pop = population
+    sub = pop[:16]
+    r = pot.relax_batch(sub, urep=UREP, rlxt=3, mitr=0, fmax=0.01)
+    atoms = sum(len(s["atmn"]) for s in sub)
+    assert r["atom_evals"] > 0 and r["atom_evals"] % atoms == 0
+    k = r["atom_evals"] // atoms
+    pairs = sum(int(pot.neighbours(s["X"], s["LAT"], s["atmn"], ND=3, NM=300)[0].sum()) for s in sub)
+    pot.profile(True, capacity=64)
+    for s in sub:
+        pot.efs(s["X"], s["LAT"], s["atmn"], ND=3, NM=300, urep=UREP)
+    trip = pot.profile_read()["triplets"]
+    pot.profile(False)
+    assert r["pairs"] == k * pairs  # the batched lists are built in FP64: the same set
+    # the batched gate tests r_jk in FP32, so a triplet within rounding of Rc may fall either way
+    assert abs(r["triplets"] - k * trip) <= max(2, 1e-5 * k * trip)

@@ -291,9 +291,11 @@ int mb_graphs(mb_potential *p, int enable);
 /* The autotuner's decisions so far: *count (at most cap) entries; entry k
  * holds the pass mode (0 descriptors, 1 energy, 2 E/F/S, 3 VJP), whether the
  * leg-table kernel ran (legs), the size bucket (N <= 2^bucket), the
- * neighbour capacity, and the chosen shape (warps per atom, atoms per CTA). */
+ * neighbour capacity, the chosen shape (warps per atom, atoms per CTA) and
+ * the leg kernel's reverse-pass layout (0 per-lane runs of list entries,
+ * 1 consecutive entries per round). */
 int mb_tune_read(const mb_potential *pot, int cap, int *count, int *mode, int *legs, int *size_bucket, int *capacity,
-                 int *wpa, int *apb);
+                 int *wpa, int *apb, int *layout);
 int mb_profile(mb_potential *pot, int enable, int capacity);
 
 /* Synchronise and report: summed duration (ms) and number of timed launches

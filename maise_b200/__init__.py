@@ -74,7 +74,7 @@ def load_library():
     lib.mb_rdf.argtypes = [c_i, c_i, _I, _I, _D, _D, c_i, c_i, c_i, c_d, c_d, c_d, c_i, _D]
     lib.mb_rdf_overlap.argtypes = [c_i, c_i, c_i, _D, _D]
     lib.mb_batch_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), _D]
-    lib.mb_tune_read.argtypes = [vp, ctypes.c_int, _I, _I, _I, _I, _I, _I, _I]
+    lib.mb_tune_read.argtypes = [vp, ctypes.c_int, _I, _I, _I, _I, _I, _I, _I, _I]
     lib.mb_atomic_mass.restype = c_d
     lib.mb_atomic_mass.argtypes = [c_i]
     lib.mb_stream.restype = vp
@@ -216,15 +216,17 @@ class Potential:
 
     def tune_table(self):
         """The autotuner's choices: list of dict(mode, legs, size_bucket,
-        capacity, wpa, apb), modes 'descriptors', 'energy', 'efs', 'vjp'."""
+        capacity, wpa, apb, layout), modes 'descriptors', 'energy', 'efs',
+        'vjp'; layout is the leg kernel's reverse pass ('runs' or 'rounds')."""
         cap = 32
-        cols = [np.zeros(cap, np.int32) for _ in range(6)]
+        cols = [np.zeros(cap, np.int32) for _ in range(7)]
         cnt = ctypes.c_int()
         self._check(self.lib.mb_tune_read(self.h, cap, ctypes.byref(cnt), *(c.ctypes.data_as(_I) for c in cols)))
         n = cnt.value
         names = ("descriptors", "energy", "efs", "vjp")
         return [dict(mode=names[int(cols[0][k])], legs=bool(cols[1][k]), size_bucket=int(cols[2][k]),
-                     capacity=int(cols[3][k]), wpa=int(cols[4][k]), apb=int(cols[5][k])) for k in range(n)]
+                     capacity=int(cols[3][k]), wpa=int(cols[4][k]), apb=int(cols[5][k]),
+                     layout="rounds" if cols[6][k] else "runs") for k in range(n)]
 
     def graphs(self, enable: bool) -> None:
         """MD chunks as CUDA graphs (default) or plain launches."""

@@ -1529,6 +1529,43 @@ __device__ __forceinline__ void leg_run_runs(const LegSmem &s, const uint2 *__re
     }
 }
 
+/* body(ent) -> the entry's force on neighbour a, over list entries
+ * [from, to), 32 consecutive entries per round (the forward pass's
+ * layout): a block's entries are ordered by a, so within a round the lanes
+ * of one a are contiguous and their b slots all differ (few conflicting
+ * b-side atomics); the a-side forces are summed per run of equal a by a
+ * segmented warp sum and added by the run's first lane. */
+template <class Body>
+__device__ __forceinline__ void leg_run_conv(const LegSmem &s, const uint2 *__restrict__ list, int from, int to,
+                                             int lane, Body body) {
+    uint2 cur = from + lane < to ? __ldg(list + from + lane) : make_uint2(0u, 0u);
+    for (int base = from; base < to; base += 32) {
+        const int t = base + lane, tn = t + 32;
+        const uint2 nxt = tn < to ? __ldg(list + tn) : make_uint2(0u, 0u);
+        const bool valid = t < to;
+        const int a = valid ? (int)(cur.x & 0xffu) : 256 + lane; /* idle lanes: segments of their own */
+        double3 g = valid ? body(cur) : make_double3(0.0, 0.0, 0.0);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double x = __shfl_down_sync(FULL, g.x, o), y = __shfl_down_sync(FULL, g.y, o),
+                         z = __shfl_down_sync(FULL, g.z, o);
+            const int an = __shfl_down_sync(FULL, a, o);
+            if (lane + o < 32 && an == a) {
+                g.x += x;
+                g.y += y;
+                g.z += z;
+            }
+        }
+        const int ap = __shfl_up_sync(FULL, a, 1);
+        if (valid && (lane == 0 || ap != a)) {
+            atomicAdd(&s.Fnb[3 * a], -g.x);
+            atomicAdd(&s.Fnb[3 * a + 1], -g.y);
+            atomicAdd(&s.Fnb[3 * a + 2], -g.z);
+        }
+        cur = nxt;
+    }
+}
+
 /* The fused descriptor / MLP / force kernel on leg tables: the stages of
  * k_efs over the triplet lists of k_trip, with every triplet's leg factors
  * read from the rows k_legs wrote (i-j and i-k from i's own rows, staged;
@@ -1536,8 +1573,10 @@ __device__ __forceinline__ void leg_run_runs(const LegSmem &s, const uint2 *__re
  * most 8 G4 exponents, zeta in {1, 2, 4, 16} or other integers, 2 lambdas. */
 /* every shape is compiled for 12 resident warps per SM (at most 170
  * registers a thread), the occupancy its shared memory also allows at the
- * alloy's neighbour counts */
-template <int NE, int WPA, int APB>
+ * alloy's neighbour counts.  RV selects the reverse pass's layout: 0 per-lane
+ * runs of entries (a-side forces in registers), 1 consecutive entries per
+ * round (b-side atomics without conflicts within a row). */
+template <int NE, int WPA, int APB, int RV>
 __global__ void __launch_bounds__(WPA * 32 * APB, 384 / (WPA * 32 * APB)) k_efs_leg(const __grid_constant__ LegArgs A) {
     constexpr int NZ = 4, NLAM = 2, NZL = 8;
     static_assert(NE == 7 || NE == 8, "leg rows hold 8 exponents");
@@ -1844,7 +1883,10 @@ __global__ void __launch_bounds__(WPA * 32 * APB, 384 / (WPA * 32 * APB)) k_efs_
                     /* the block's entries in WPA contiguous parts, one per warp */
                     const int from = tb[blkid], to = tb[blkid + 1], per = (to - from + WPA - 1) / WPA;
                     const int lo = min(to, from + warp * per), hi = min(to, lo + per);
-                    leg_run_runs(s, tl, lo, hi, lane, body);
+                    if constexpr (RV == 0)
+                        leg_run_runs(s, tl, lo, hi, lane, body);
+                    else
+                        leg_run_conv(s, tl, lo, hi, lane, body);
                 }
                 group_sync<WPA>();
             }
@@ -2291,16 +2333,18 @@ extern "C" int mbk_legs_usable(const mb_dev *d, const mb_model *m, int N, const 
     return leg_model_ok(m) ? 1 : 0;
 }
 
-static const EfsShape kLegShapes[] = {{1, 4}, {1, 2}, {2, 1}, {4, 1}};
-#define MB_NLEGSHAPES 4
+/* shapes 0-3 with the per-lane-run reverse layout, 4-7 the same shapes
+ * with the consecutive-entry layout */
+static const EfsShape kLegShapes[] = {{1, 4}, {1, 2}, {2, 1}, {4, 1}, {1, 4}, {1, 2}, {2, 1}, {4, 1}};
+#define MB_NLEGSHAPES 8
 
 static size_t leg_group_bytes(const mb_model *m, int capNB, int wpa) {
     return leg_smem_bytes(capNB, m->P.D, m->P.ng2, wpa);
 }
 
-template <int NE, int WPA, int APB>
+template <int NE, int WPA, int APB, int RV>
 static int launch_leg(const LegArgs &a, cudaStream_t st) {
-    auto kern = k_efs_leg<NE, WPA, APB>;
+    auto kern = k_efs_leg<NE, WPA, APB, RV>;
     const size_t smem = a.smem_group * APB;
     static size_t configured[MB_MAX_DEVICES_K] = {0};
     int dev = 0;
@@ -2327,17 +2371,25 @@ static int launch_leg_pass(const mb_dev *d, const mb_model *m, int shape, LegArg
     int rc;
     if (m->P.ne <= 7) {
         switch (shape) {
-            case 0: rc = launch_leg<7, 1, 4>(a, st); break;
-            case 1: rc = launch_leg<7, 1, 2>(a, st); break;
-            case 2: rc = launch_leg<7, 2, 1>(a, st); break;
-            default: rc = launch_leg<7, 4, 1>(a, st); break;
+            case 0: rc = launch_leg<7, 1, 4, 0>(a, st); break;
+            case 1: rc = launch_leg<7, 1, 2, 0>(a, st); break;
+            case 2: rc = launch_leg<7, 2, 1, 0>(a, st); break;
+            case 3: rc = launch_leg<7, 4, 1, 0>(a, st); break;
+            case 4: rc = launch_leg<7, 1, 4, 1>(a, st); break;
+            case 5: rc = launch_leg<7, 1, 2, 1>(a, st); break;
+            case 6: rc = launch_leg<7, 2, 1, 1>(a, st); break;
+            default: rc = launch_leg<7, 4, 1, 1>(a, st); break;
         }
     } else {
         switch (shape) {
-            case 0: rc = launch_leg<8, 1, 4>(a, st); break;
-            case 1: rc = launch_leg<8, 1, 2>(a, st); break;
-            case 2: rc = launch_leg<8, 2, 1>(a, st); break;
-            default: rc = launch_leg<8, 4, 1>(a, st); break;
+            case 0: rc = launch_leg<8, 1, 4, 0>(a, st); break;
+            case 1: rc = launch_leg<8, 1, 2, 0>(a, st); break;
+            case 2: rc = launch_leg<8, 2, 1, 0>(a, st); break;
+            case 3: rc = launch_leg<8, 4, 1, 0>(a, st); break;
+            case 4: rc = launch_leg<8, 1, 4, 1>(a, st); break;
+            case 5: rc = launch_leg<8, 1, 2, 1>(a, st); break;
+            case 6: rc = launch_leg<8, 2, 1, 1>(a, st); break;
+            default: rc = launch_leg<8, 4, 1, 1>(a, st); break;
         }
     }
     if (e1) mbk_record(e1, st);
@@ -2363,43 +2415,52 @@ static int tune_key(const mb_dev *d, int N, int mode) {
     return (mode << 28) | ((d->legs_on ? 1 : 0) << 26) | (bucket << 20) | (d->capNB & 0xfffff);
 }
 
-static int tune_leg(mb_dev *d, const mb_model *m, int N, int mode, const LegArgs &a, cudaStream_t st) {
+/* Decision for a pass that may run on leg tables: the four leg shapes and
+ * the shapes of k_efs are each timed once (after an untimed launch) and the
+ * fastest kept, 16 + shape for the leg path, shape for k_efs.  Small
+ * structures (a few dozen atoms: one CTA per atom, most SMs idle) can favour
+ * k_efs's many-warp shapes; large ones the leg path. */
+static int tune_family(mb_dev *d, const mb_model *m, int N, int mode, const LegArgs &la, const EfsArgs &a,
+                       cudaStream_t st) {
     const int key = tune_key(d, N, mode);
     for (int k = 0; k < d->tune_n; k++)
         if (d->tune_key[k] == key) return d->tune_val[k];
+    int best = 16;
     if (d->tune_fixed >= 0) {
-        /* a forced shape is recorded as the decision for this key */
-        const int v = d->tune_fixed < MB_NLEGSHAPES ? d->tune_fixed : 0;
-        if (d->tune_n < MB_TUNE_SLOTS) {
-            d->tune_key[d->tune_n] = key;
-            d->tune_val[d->tune_n++] = v;
+        /* a forced shape (of the leg path) is recorded as the decision for this key */
+        best = 16 + (d->tune_fixed < MB_NLEGSHAPES ? d->tune_fixed : 0);
+    } else {
+        LegArgs tl = la;
+        EfsArgs te = a;
+        tl.counters = nullptr;
+        te.counters = nullptr;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        float best_ms = 1e30f;
+        for (int c = 0; c < MB_NLEGSHAPES + MB_NSHAPES; c++) {
+            const bool leg = c < MB_NLEGSHAPES;
+            const int sh = leg ? c : c - MB_NLEGSHAPES;
+            const size_t need = leg ? leg_group_bytes(m, la.cap, kLegShapes[sh].wpa) * kLegShapes[sh].apb + LEG_STATIC_SMEM
+                                    : group_bytes(m, a.cap, kShapes[sh].wpa) * kShapes[sh].apb + EFS_STATIC_SMEM;
+            if (need > 227 * 1024) continue;
+            float ms = 1e30f;
+            int bad = 0;
+            for (int rep = 0; rep < 2 && !bad; rep++) {
+                if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
+                bad = leg ? launch_leg_pass(d, m, sh, tl, st, rep ? e0 : nullptr, rep ? e1 : nullptr)
+                          : launch_any(m, sh, te, st, rep ? e0 : nullptr, rep ? e1 : nullptr);
+            }
+            if (!bad && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = leg ? 16 + sh : sh;
+            }
         }
-        return v;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaGetLastError();
     }
-    LegArgs t = a;
-    t.counters = nullptr;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    int best = 0;
-    float best_ms = 1e30f;
-    for (int sh = 0; sh < MB_NLEGSHAPES; sh++) {
-        if (leg_group_bytes(m, a.cap, kLegShapes[sh].wpa) * kLegShapes[sh].apb + LEG_STATIC_SMEM > 227 * 1024) continue;
-        float ms = 1e30f;
-        int bad = 0;
-        for (int rep = 0; rep < 2 && !bad; rep++) {
-            if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
-            bad = launch_leg_pass(d, m, sh, t, st, rep ? e0 : nullptr, rep ? e1 : nullptr);
-        }
-        if (!bad && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = sh;
-        }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaGetLastError();
     if (d->tune_n < MB_TUNE_SLOTS) {
         d->tune_key[d->tune_n] = key;
         d->tune_val[d->tune_n] = best;
@@ -2476,6 +2537,7 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
     a.counters = d->counters;
     a.smem_group = 0;
     cudaMemsetAsync(d->EU, 0, sizeof(double) * N, st);
+    int fam = -1; /* k_efs shape chosen against the leg path */
     if (d->legs_on) {
         LegArgs la;
         la.N = N;
@@ -2501,20 +2563,23 @@ extern "C" int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode
         la.counters = d->counters;
         la.smem_group = 0;
         la.P = m->P;
-        const int shape = tune_leg(d, m, N, mode, la, st);
-        d->last_shape = 16 + shape;
-        cudaEvent_t e0 = 0, e1 = 0;
-        if (d->ev_on && d->ev_n < d->ev_cap) {
-            e0 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n];
-            e1 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n + 1];
-            d->ev_n++;
+        const int v = tune_family(d, m, N, mode, la, a, st);
+        if (v >= 16) {
+            d->last_shape = v;
+            cudaEvent_t e0 = 0, e1 = 0;
+            if (d->ev_on && d->ev_n < d->ev_cap) {
+                e0 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n];
+                e1 = ((cudaEvent_t *)d->ev_pool)[2 * d->ev_n + 1];
+                d->ev_n++;
+            }
+            if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
+            const int rc = launch_leg_pass(d, m, v - 16, la, st, e0, e1);
+            (*launches) += 3;
+            return rc;
         }
-        if (mode == MB_MODE_EFS || mode == MB_MODE_VJP) cudaMemsetAsync(d->F, 0, sizeof(double) * 3 * N, st);
-        const int rc = launch_leg_pass(d, m, shape, la, st, e0, e1);
-        (*launches) += 3;
-        return rc;
+        fam = v;
     }
-    int shape = tune_shape(d, m, N, mode, a, st);
+    int shape = fam >= 0 ? fam : tune_shape(d, m, N, mode, a, st);
     d->last_shape = shape;
     cudaEvent_t e0 = 0, e1 = 0;
     if (d->ev_on && d->ev_n < d->ev_cap) {

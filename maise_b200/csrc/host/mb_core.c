@@ -257,18 +257,21 @@ int mb_batch_stats(const mb_potential *p, long long *evals, double *ms) {
 }
 
 int mb_tune_read(const mb_potential *p, int cap, int *count, int *mode, int *legs, int *size_bucket, int *capacity,
-                 int *wpa, int *apb) {
+                 int *wpa, int *apb, int *layout) {
     int k, n;
     if (!p || cap < 0 || !count) return fail(MB_ERR_ARG, "bad arguments");
     n = p->d.tune_n < cap ? p->d.tune_n : cap;
     *count = n;
     for (k = 0; k < n; k++) {
-        const int key = p->d.tune_key[k], lg = (key >> 26) & 1;
+        /* a key with the leg path usable holds 16 + shape when the leg kernel
+         * won and a k_efs shape otherwise */
+        const int key = p->d.tune_key[k], v = p->d.tune_val[k], lg = ((key >> 26) & 1) && v >= 16;
         mode[k] = key >> 28;
         legs[k] = lg;
         size_bucket[k] = (key >> 20) & 0x3f;
         capacity[k] = key & 0xfffff;
-        if (mbk_shape_dims(lg, p->d.tune_val[k], &wpa[k], &apb[k])) wpa[k] = apb[k] = 0;
+        if (mbk_shape_dims(lg, lg ? v - 16 : v, &wpa[k], &apb[k])) wpa[k] = apb[k] = 0;
+        layout[k] = lg && v - 16 >= 4; /* leg shapes 4-7: reverse pass over consecutive entries */
     }
     return MB_OK;
 }

@@ -222,15 +222,16 @@ def test_capacity_growth_between_calls(mb, tmp_path):
 
 @pytest.mark.parametrize("shape", [0, 1, 2])
 def test_every_kernel_shape_matches_oracle_at_large_capacity(mb, tmp_path, monkeypatch, shape):
-    """Each warps-per-atom shape forced in turn (the autotuner would skip a
-    shape whose launch fails), with the neighbour capacity reserved at 128
-    so that the wide shapes need more than the 48 KB default of shared
-    memory."""
+    """Each warps-per-atom shape of k_efs (the general fused kernel, leg
+    tables off) forced in turn (the autotuner would skip a shape whose
+    launch fails), with the neighbour capacity reserved at 128 so that the
+    wide shapes need more than the 48 KB default of shared memory."""
     from maise_b200 import workloads
 
     w = workloads.random_alloy(n=3, a=3.8, seed=8, jitter=0.08)
     d = _model_for(tmp_path, w)
     monkeypatch.setenv("MAISE_B200_SHAPE", str(shape))
+    monkeypatch.setenv("MAISE_B200_LEGS", "0")
     pot, o = mb.Potential(d + "/model"), Oracle(d + "/model")
     pot.reserve(len(w["atmn"]), 128)
     r = pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=200)

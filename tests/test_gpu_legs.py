@@ -14,11 +14,17 @@ from oracle import Oracle
 pytestmark = pytest.mark.gpu
 
 
-def _pots(monkeypatch, path):
+def _pots(monkeypatch, path, force_legs=True):
+    """(leg path, general path): the first handle is held to the leg kernel
+    (a fixed leg shape; the autotuner may otherwise prefer k_efs for small
+    structures), the second cannot use it."""
     import maise_b200
 
     monkeypatch.setenv("MAISE_B200_LEGS", "1")
+    if force_legs:
+        monkeypatch.setenv("MAISE_B200_SHAPE", "2")
     a = maise_b200.Potential(path)
+    monkeypatch.delenv("MAISE_B200_SHAPE", raising=False)
     monkeypatch.setenv("MAISE_B200_LEGS", "0")
     b = maise_b200.Potential(path)
     monkeypatch.delenv("MAISE_B200_LEGS")
@@ -69,8 +75,9 @@ def test_leg_path_matches_general_path_and_oracle(tmp_path, monkeypatch, name):
 
 
 def test_leg_path_every_shape(tmp_path, monkeypatch):
-    """Every kernel shape of the leg path (warps per atom x atoms per block)
-    gives the same forces; the autotuner only chooses among them."""
+    """Every kernel shape of the leg path (warps per atom x atoms per block,
+    each with both reverse-pass layouts) gives the same forces; the
+    autotuner only chooses among them."""
     import maise_b200
     from maise_b200 import models, workloads
 
@@ -78,7 +85,7 @@ def test_leg_path_every_shape(tmp_path, monkeypatch):
     path = str(tmp_path / "model")
     models.random_model(path, [29, 46, 47], models.Basis(), (w["X"], w["LAT"], w["atmn"], 3), seed=2)
     want = Oracle(path).efs(w["X"], w["LAT"], w["atmn"], 3, NM=300)
-    for shape in range(4):
+    for shape in range(8):
         monkeypatch.setenv("MAISE_B200_SHAPE", str(shape))
         pot = maise_b200.Potential(path)
         r = pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=300)
@@ -95,15 +102,16 @@ def test_tune_table_records_the_chosen_shapes(tmp_path, monkeypatch):
     w = dict(_cases())["alloy"]
     path = str(tmp_path / "model")
     models.random_model(path, [29, 46, 47], models.Basis(), (w["X"], w["LAT"], w["atmn"], 3), seed=4)
-    legs, plain = _pots(monkeypatch, path)
-    for pot, uses_legs in ((legs, True), (plain, False)):
+    legs, plain = _pots(monkeypatch, path, force_legs=False)
+    for pot, can_use_legs in ((legs, True), (plain, False)):
         pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=300)
         pot.energy(w["X"], w["LAT"], w["atmn"], ND=3, NM=300)
         tt = pot.tune_table()
         modes = {e["mode"] for e in tt}
         assert {"efs", "energy"} <= modes
         for e in tt:
-            assert e["legs"] == uses_legs
+            # with leg tables available the tuner picks the faster kernel family
+            assert e["legs"] in ((True, False) if can_use_legs else (False,))
             assert e["size_bucket"] == 8  # 256 atoms
             assert e["wpa"] in (1, 2, 4, 8) and e["apb"] in (1, 2, 4)
         n = len(tt)

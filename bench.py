@@ -348,6 +348,10 @@ def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs
     top = np.argsort(truth_plain, kind="stable")[:ntop]
     recall_plain = float(in_kept[sample[top]].mean())
     sur.close()
+    try:
+        fixed = fixed_composition_generation(pot, local, urep=urep, mitr=mitr, fmax=fmax, keep=keep, epochs=epochs)
+    except Exception as e:  # noqa: BLE001 -- reported in the field, the generation's own numbers stand
+        fixed = {"error": f"{type(e).__name__}: {e}"}
     pot.close()
     return {"workload": GEN_WORKLOAD, "offspring": n_gen, "train_pairs": n_train, "keep": keep,
             "recall_top10": recall(pred, truth, keep), "recall_top10_by_unrelaxed_energy": recall(e0, truth, keep),
@@ -367,7 +371,37 @@ def surrogate_generation(local, td, n_train=20000, n_gen=4096, keep=0.25, epochs
                                 "triplets": rk["triplets"] / max(1, ra["triplets"]),
                                 "kernel_time": rk["ms"] / max(1e-9, ra["ms"])},
             "train_data_relax_s": t_data, "fit_s": t_fit, "epochs": epochs, "final_loss": float(loss[-1]),
-            "judge": "batched relax of every offspring (FP32 descriptors/MLP, FP64 BFGS)"}
+            "judge": "batched relax of every offspring (FP32 descriptors/MLP, FP64 BFGS)",
+            "fixed_composition": fixed}
+
+
+def fixed_composition_generation(pot, local, urep, mitr, fmax, keep, epochs, n_train=4096, n_gen=1024):
+    """The screen where composition says nothing: every offspring Cu:Pd:Ag
+    1:1:1 (18-48 atoms), a surrogate trained on 4096 relaxed offspring of
+    that composition, recall of the best 10% of 1024 others against ranking
+    by unrelaxed enthalpy and against random."""
+    from maise_b200 import workloads
+    from maise_b200.surrogate import Surrogate, recall
+
+    spc = (29, 46, 47)
+    kw = dict(nmin=18, nmax=48, species=spc, composition=(1, 1, 1))
+    train = workloads.ea_population_chunked(n_train, seed=21, **kw)
+    gen = workloads.ea_population_chunked(n_gen, seed=22, **kw)
+    rt = pot.relax_batch(train, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
+    ra = pot.relax_batch(gen, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
+    nt = np.array([len(s["atmn"]) for s in train])
+    ng = np.array([len(s["atmn"]) for s in gen])
+    sur = Surrogate(3, device=local)
+    sur.fit(sur.features(train), rt["H"] / nt, epochs=epochs, batch=256, lr=1e-3)
+    pred = sur.screen(gen)
+    sur.close()
+    truth = ra["H"] / ng
+    e0 = np.array([pot.energy(s["X"], s["LAT"], s["atmn"], ND=3, NM=300, urep=urep)["H"] for s in gen]) / ng
+    return {"offspring": n_gen, "train_pairs": n_train, "composition": "Cu:Pd:Ag 1:1:1, 18-48 atoms",
+            "recall_top10": recall(pred, truth, keep), "recall_top10_by_unrelaxed_energy": recall(e0, truth, keep),
+            "recall_top10_random_expectation": keep,
+            "mae_ev_per_atom": float(np.abs(pred - truth).mean()),
+            "spread_ev_per_atom": float(truth.std())}
 
 
 def _efs_rate(pot, w, ND, calls, NM):
@@ -500,8 +534,9 @@ def particle_leg(local, td, peak, md_steps=500, cpu=True):
 
 def profile_case(case):
     """Small cases sized for an ncu capture (a few MB on the device):
-    md           the 4000-atom workload: the bench's 20 settle steps, then 3 NVT
-                 steps at the settled neighbour counts (descriptor-pass launches)
+    md           the 4000-atom workload: the bench's 20 settle steps, then 10 NVT
+                 steps at the settled neighbour counts (descriptor-pass launches;
+                 the autotuner's trial launches all come before the last 10)
     relax-batch  64 Mg-Ca structures of the population relax, 20 BFGS iterations
     surrogate    features of 512 Cu-Pd-Ag offspring and 5 training epochs"""
     import maise_b200
@@ -513,7 +548,7 @@ def profile_case(case):
         pot = maise_b200.Potential(make_model(td, w, basis))
         V = maxwell([atomic_mass(w["spcz"][s]) for s in w["atmn"]], 600.0, seed=7)
         st = pot.md_nvt(w["X"], w["LAT"], w["atmn"], V, 600.0, nsteps=SETTLE_STEPS, NM=100, trace=False)
-        pot.md_nvt(st["X"], w["LAT"], w["atmn"], st["V"], 600.0, nsteps=3, NM=100, xi=st["xi"], trace=False)
+        pot.md_nvt(st["X"], w["LAT"], w["atmn"], st["V"], 600.0, nsteps=10, NM=100, xi=st["xi"], trace=False)
     elif case == "relax-batch":
         pop = workloads.ea_population(count=64, seed=3)
         pot = maise_b200.Potential(_binding_model(td, "pop", pop, (12, 20), 5))

@@ -1209,20 +1209,26 @@ __global__ void __launch_bounds__(WPA * 32 * APB, APB >= 4 ? 2 : 1) k_efs(EfsArg
 #define LEG_PER_LANE (MB_LEG_MAX_CAP / 32)
 #define LEG_HASH 256 /* hash slots per atom: at least twice the neighbour capacity */
 
-__device__ __forceinline__ int sx5(unsigned v) { return (int)((v & 31u) ^ 16u) - 16; }
+
+__device__ __forceinline__ unsigned hash_slot(unsigned key) { return (key * 0x9E3779B1u) >> 24; }
 
 /* One warp per atom: sort the atom's entries stably by the neighbour's
  * species (in place: nj, nk, nd), record where each species starts
- * (nso[4i+s]; nso[4i+3] = count), and write each entry's leg row with the
+ * (nso[4i+s]; nso[4i+3] = count), write each entry's leg row with the
  * forward parameters of the pair (i, j): exp(-eta_e r^2) for e < ne (0
- * above), fc(r) and fc'(r)/r at the G4 cutoff. */
+ * above), fc(r) and fc'(r)/r at the G4 cutoff, and put the entries' keys
+ * (atom, image) with their sorted slots into the atom's hash
+ * gh[i * LEG_HASH ..] (linear probing), where k_trip looks a neighbour's
+ * neighbours up. */
 __global__ void k_legs(int N, int cap, const int *__restrict__ nn, int *__restrict__ nj, unsigned *__restrict__ nk,
                        double4 *__restrict__ nd, const int *__restrict__ spc, const mb_params *__restrict__ Pg,
-                       double *__restrict__ leg, int *__restrict__ nso) {
+                       double *__restrict__ leg, int *__restrict__ nso, uint2 *__restrict__ gh) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= N) return;
     const int i = warp, n = nn[i], s0 = spc[i], ne = Pg->ne;
     const size_t row = (size_t)i * cap;
+    uint2 *hash = gh + (size_t)i * LEG_HASH;
+    for (int t = lane; t < LEG_HASH; t += 32) hash[t] = make_uint2(0xffffffffu, 0u);
     int jv[LEG_PER_LANE], spv[LEG_PER_LANE];
     unsigned kv[LEG_PER_LANE];
     double4 dv[LEG_PER_LANE];
@@ -1264,6 +1270,16 @@ __global__ void k_legs(int N, int cap, const int *__restrict__ nn, int *__restri
             nj[row + dst] = jv[q];
             nk[row + dst] = kv[q];
             nd[row + dst] = dv[q];
+            {
+                unsigned h = hash_slot(kv[q]);
+                for (int probe = 0; probe < LEG_HASH; probe++) {
+                    if (atomicCAS(&hash[h].x, 0xffffffffu, kv[q]) == 0xffffffffu) {
+                        hash[h].y = (unsigned)dst;
+                        break;
+                    }
+                    h = (h + 1u) & (LEG_HASH - 1u);
+                }
+            }
             const int p = s0 * s0 + spv[q] * spv[q];
             const double r = dv[q].w;
             double f, df;
@@ -1340,59 +1356,53 @@ __device__ inline LegSmem leg_carve(char *base, int cap, int D, int ng2, int war
     return s;
 }
 
-__device__ __forceinline__ unsigned hash_slot(unsigned key) { return (key * 0x9E3779B1u) >> 24; }
 
 /* Triplet lists of the leg path: one warp per atom i, TRIP_WARPS atoms per
- * CTA.  The warp stages i's entries in relative-species order (position u,
- * the order k_efs_leg stages them in: relative species v holds absolute
- * species (s0 + v) % ns) with each entry's key (atom << 15 | image), its
- * atom j and the species starts of j's list, and puts the keys into a hash.
- * For every species block (alpha <= beta) it then walks, for each entry a
- * of relative species alpha, the entries c of j's own list whose atom has
- * absolute species (s0 + beta) % ns, 32 candidates per round: the entry's
- * atom k at image key(a) + key(c) is looked up among i's keys, and a found
- * slot b > a makes (a, b) a triplet with r_ij, r_ik and r_jk below Rc
- * (each (k, image) of j's list is a distinct image relative to i, so a
- * pair (a, b) is found at most once and a list never exceeds
- * tcap = cap (cap - 1) / 2).  Accepted entries {a | b << 8, row} -- row =
- * j cap + c, the j-k leg row -- are written in candidate order (a
- * ascending, then c), so every list is
- * deterministic; tboff[8 i + blk] holds the start of each block and
- * tboff[8 i + nblk] the end.  counters[1] (if set) receives the number of
- * triplets. */
+ * CTA.  PRS_BP takes the triplet (j, k) of i when NDX[i][j] and NDX[i][k]
+ * are below the G4 cutoff and so is ndx[i][j][k] = |DX_j - DX_k|, both
+ * displacements from i's list (src/nprs.c:528-537, src/cell.c:175-181).
+ * The warp stages i's entries in relative-species order (position u, the
+ * order k_efs_leg stages them in: relative species v holds absolute
+ * species (s0 + v) % ns) and walks, per species block (alpha <= beta), the
+ * pairs (a, b), b > a, 32 per round, with that test: the squared distance
+ * summed without contraction as the reference forms it, compared with the
+ * threshold for which sqrt(s) < Rc holds exactly.  An accepted pair's j-k
+ * leg row is the entry of k (its atom at the image shift(b) - shift(a)) in
+ * j's own list, found in j's hash (k_legs); a pair whose k is not in j's
+ * list lies within rounding of the cutoff, where fc vanishes, and is left
+ * out.  Entries {a | b << 8, j cap + c} are written in pair order (a, then
+ * b), so every list is deterministic and at most cap (cap - 1) / 2 long;
+ * tboff[8 i + blk] holds each block's start and tboff[8 i + nblk] the end.
+ * counters[1] (if set) receives the number of triplets. */
 #define TRIP_WARPS 8
 
 /* The 15-bit image field of an entry key (three 5-bit two's-complement
- * shifts) spread into 7-bit fields with the bias +16, so that the image of
- * a sum of two displacements is one integer add: field t = x_a + x_c + 48,
- * in [32, 63] exactly when the summed shift lies in [-16, 15]. */
+ * shifts) as three biased (x + 16) 7-bit fields, so that shifts add and
+ * subtract as integers. */
 __device__ __forceinline__ unsigned spread_img(unsigned key) {
     const unsigned f = (key & 0x7fffu) ^ 0x4210u; /* x + 16 per field */
     return (f & 31u) | ((f & (31u << 5)) << 2) | ((f & (31u << 10)) << 4);
 }
-#define IMG_BIAS (16u | (16u << 7) | (16u << 14))
+#define IMG_48 (48u | (48u << 7) | (48u << 14))
 #define IMG_BIT5 ((1u << 5) | (1u << 12) | (1u << 19))
 #define IMG_BIT6 ((1u << 6) | (1u << 13) | (1u << 20))
 
 __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tcap, int ns, const int *__restrict__ nn,
                                                           const int *__restrict__ nj, const unsigned *__restrict__ nk,
-                                                          const int *__restrict__ nso, const int *__restrict__ spc,
-                                                          uint2 *__restrict__ trip, int *__restrict__ tboff,
-                                                          unsigned long long *counters) {
-    __shared__ uint2 hsh[TRIP_WARPS][LEG_HASH];
-    /* per staged entry a: its atom j, j cap (j's list row), the spread image
-     * of its key plus the bias, and (per species block) where j's entries of
-     * the block's second species start and how many there are */
-    __shared__ int sj[TRIP_WARPS][MB_LEG_MAX_CAP], srow[TRIP_WARPS][MB_LEG_MAX_CAP];
-    __shared__ unsigned simg[TRIP_WARPS][MB_LEG_MAX_CAP];
-    __shared__ int sst[TRIP_WARPS][MB_LEG_MAX_CAP], slen[TRIP_WARPS][MB_LEG_MAX_CAP];
+                                                          const double4 *__restrict__ nd, const int *__restrict__ nso,
+                                                          const int *__restrict__ spc, const mb_params *__restrict__ Pg,
+                                                          const uint2 *__restrict__ gh, uint2 *__restrict__ trip,
+                                                          int *__restrict__ tboff, unsigned long long *counters) {
+    __shared__ double4 sd[TRIP_WARPS][MB_LEG_MAX_CAP];
+    __shared__ unsigned skey[TRIP_WARPS][MB_LEG_MAX_CAP];
+    __shared__ int sj[TRIP_WARPS][MB_LEG_MAX_CAP];
     __shared__ int sseg[TRIP_WARPS][8];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * TRIP_WARPS + w;
     if (i >= N) return; /* whole warps; nothing below synchronises the CTA */
-    uint2 *hash = hsh[w];
-    int *js = sj[w], *rowj = srow[w], *st = sst[w], *len = slen[w], *seg = sseg[w];
-    unsigned *img = simg[w];
+    double4 *d = sd[w];
+    unsigned *key = skey[w];
+    int *js = sj[w], *seg = sseg[w];
     const int n = nn[i], s0 = spc[i];
     const size_t row = (size_t)i * cap;
     if (lane < 4) {
@@ -1406,26 +1416,15 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
         seg[v] = c;
         seg[4 + v] = v < ns ? o : n;
     }
-    for (int t = lane; t < LEG_HASH; t += 32) hash[t] = make_uint2(0xffffffffu, 0u);
     __syncwarp();
     for (int u = lane; u < n; u += 32) {
         int v = 0;
         while (v + 1 < ns && u >= seg[4 + v + 1]) v++;
         const int sa = (s0 + v) % ns;
         const int t = nso[4 * i + sa] + (u - seg[4 + v]);
-        const int j = nj[row + t];
-        const unsigned k = nk[row + t];
-        js[u] = j;
-        rowj[u] = j * cap;
-        img[u] = spread_img(k) + IMG_BIAS;
-        unsigned h = hash_slot(k);
-        for (int probe = 0; probe < LEG_HASH; probe++) {
-            if (atomicCAS(&hash[h].x, 0xffffffffu, k) == 0xffffffffu) {
-                hash[h].y = (unsigned)u;
-                break;
-            }
-            h = (h + 1u) & (LEG_HASH - 1u);
-        }
+        d[u] = nd[row + t];
+        key[u] = nk[row + t];
+        js[u] = nj[row + t];
     }
     __syncwarp();
     uint2 *out = trip + (size_t)i * tcap;
@@ -1433,57 +1432,61 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
     for (int al = 0; al < ns; al++)
         for (int be = al; be < ns; be++, blkid++) {
             if (lane == 0) tboff[8 * i + blkid] = pos;
-            const int sb = (s0 + be) % ns, a_lo = seg[4 + al], a_hi = a_lo + seg[al];
-            for (int a = a_lo + lane; a < a_hi; a += 32) {
-                const int *o = nso + 4 * (size_t)js[a];
-                st[a] = o[sb];
-                len[a] = o[sb + 1] - o[sb];
-            }
-            __syncwarp();
-            /* the lane's candidate (ca, cc): entry cc of j's species-sb entries, j = atom of i's entry ca */
-            int ca = a_lo, cc = lane;
-            while (ca < a_hi && cc >= len[ca]) {
-                cc -= len[ca];
-                ca++;
-            }
-            for (;;) {
-                const bool live = ca < a_hi;
-                if (!__any_sync(FULL, live)) break;
+            const int sj_ = (s0 + al) % ns, sk_ = (s0 + be) % ns;
+            const int p01 = s0 * s0 + sj_ * sj_, p02 = s0 * s0 + sk_ * sk_, p12 = sj_ * sj_ + sk_ * sk_;
+            const double R01 = __ldg(&Pg->f_rc4[p01]), R02 = __ldg(&Pg->f_rc4[p02]);
+            const double thr = __ldg(&Pg->f_rc4thr[p12]);
+            const int na = seg[al], nb = seg[be], oa = seg[4 + al], ob = seg[4 + be];
+            const bool tri = al == be;
+            const int C = tri ? na * (na - 1) / 2 : na * nb;
+            const float tb = (float)(2 * na - 1);
+            for (int base = 0; base < C; base += 32) {
+                const int c = base + lane;
                 bool ok = false;
                 uint2 ent = make_uint2(0u, 0u);
-                if (live) {
-                    const unsigned r = (unsigned)(rowj[ca] + st[ca] + cc);
-                    const unsigned kc = __ldg(nk + r);
-                    const unsigned t = spread_img(kc) + img[ca];
-                    if ((t & IMG_BIT6) == 0u && (t & IMG_BIT5) == IMG_BIT5) {
-                        /* back to three 5-bit two's-complement fields */
-                        const unsigned f = (t & 31u) | ((t >> 2) & (31u << 5)) | ((t >> 4) & (31u << 10));
-                        const unsigned kk = (kc & ~0x7fffu) | (f ^ 0x4210u);
-                        unsigned h = hash_slot(kk);
-                        int b = -1;
-                        for (int probe = 0; probe < LEG_HASH; probe++) {
-                            const uint2 e = hash[h];
-                            if (e.x == kk) {
-                                b = (int)e.y;
-                                break;
+                if (c < C) {
+                    int r, col;
+                    if (tri) {
+                        /* row r of the strict upper triangle starts at r (2 na - r - 1) / 2 */
+                        r = __float2int_rz(0.5f * (tb - sqrtf(fmaxf(tb * tb - 8.0f * (float)c, 0.0f))));
+                        r = min(max(r, 0), na - 2);
+                        while (r > 0 && r * (2 * na - r - 1) / 2 > c) r--;
+                        while (r < na - 2 && (r + 1) * (2 * na - r - 2) / 2 <= c) r++;
+                        col = c - r * (2 * na - r - 1) / 2 + r + 1;
+                    } else {
+                        r = c / nb;
+                        col = c - r * nb;
+                    }
+                    const int a = oa + r, b = ob + col;
+                    const double4 da = d[a], db = d[b];
+                    const double dx = xsub(da.x, db.x), dy = xsub(da.y, db.y), dz = xsub(da.z, db.z);
+                    const double s2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+                    if (da.w < R01 && db.w < R02 && s2 < thr) {
+                        const unsigned ka = key[a], kb = key[b];
+                        const unsigned t = IMG_48 + spread_img(kb) - spread_img(ka);
+                        if ((t & IMG_BIT6) == 0u && (t & IMG_BIT5) == IMG_BIT5) {
+                            const unsigned f = (t & 31u) | ((t >> 2) & (31u << 5)) | ((t >> 4) & (31u << 10));
+                            const unsigned kk = (kb & ~0x7fffu) | (f ^ 0x4210u); /* k at its image relative to j */
+                            const int j = js[a];
+                            const uint2 *hj = gh + (size_t)j * LEG_HASH;
+                            unsigned h = hash_slot(kk);
+                            for (int probe = 0; probe < LEG_HASH; probe++) {
+                                const uint2 e = __ldg(hj + h);
+                                if (e.x == kk) {
+                                    ok = true;
+                                    ent = make_uint2((unsigned)a | ((unsigned)b << 8), (unsigned)j * (unsigned)cap + e.y);
+                                    break;
+                                }
+                                if (e.x == 0xffffffffu) break;
+                                h = (h + 1u) & (LEG_HASH - 1u);
                             }
-                            if (e.x == 0xffffffffu) break;
-                            h = (h + 1u) & (LEG_HASH - 1u);
                         }
-                        ok = b > ca;
-                        ent = make_uint2((unsigned)ca | ((unsigned)b << 8), r);
                     }
                 }
                 const unsigned m = __ballot_sync(FULL, ok);
                 if (ok) out[pos + __popc(m & ((1u << lane) - 1u))] = ent;
                 pos += __popc(m);
-                cc += 32;
-                while (ca < a_hi && cc >= len[ca]) {
-                    cc -= len[ca];
-                    ca++;
-                }
             }
-            __syncwarp();
         }
     if (lane == 0) {
         tboff[8 * i + blkid] = pos;
@@ -2326,7 +2329,7 @@ extern "C" int mbk_legs_model(const mb_model *m) { return leg_model_ok(m) ? 1 : 
  * qualifies, the tables are allocated, and every entry key fits (atom
  * index in 17 bits, images within +-15, neighbour capacity <= 128) */
 extern "C" int mbk_legs_usable(const mb_dev *d, const mb_model *m, int N, const mb_cell *c) {
-    if (!d->nk || !d->leg || !d->nso || !d->trip || !d->tboff) return 0;
+    if (!d->nk || !d->leg || !d->nso || !d->trip || !d->tboff || !d->lhash) return 0;
     if (N >= MB_LEG_MAX_ATOMS || d->capNB > MB_LEG_MAX_CAP) return 0;
     for (int q = 0; q < 3; q++)
         if (c->Nq[q] > MB_LEG_MAX_IMAGE) return 0;
@@ -2365,9 +2368,10 @@ static int launch_leg_pass(const mb_dev *d, const mb_model *m, int shape, LegArg
     a.smem_group = leg_group_bytes(m, a.cap, kLegShapes[shape].wpa);
     if (e0) mbk_record(e0, st);
     k_legs<<<(a.N + 3) / 4, 128, 0, st>>>(a.N, a.cap, d->nn, d->nj, d->nk, (double4 *)d->nd, d->spc, d->params,
-                                         d->leg, d->nso);
+                                         d->leg, d->nso, (uint2 *)d->lhash);
     k_trip<<<(a.N + TRIP_WARPS - 1) / TRIP_WARPS, 32 * TRIP_WARPS, 0, st>>>(
-        a.N, a.cap, d->tcap, m->P.nspc, d->nn, d->nj, d->nk, d->nso, d->spc, (uint2 *)d->trip, d->tboff, a.counters);
+        a.N, a.cap, d->tcap, m->P.nspc, d->nn, d->nj, d->nk, (const double4 *)d->nd, d->nso, d->spc, d->params,
+        (const uint2 *)d->lhash, (uint2 *)d->trip, d->tboff, a.counters);
     int rc;
     if (m->P.ne <= 7) {
         switch (shape) {

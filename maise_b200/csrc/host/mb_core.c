@@ -175,7 +175,7 @@ int mb_open(const char *model_path, int device, mb_potential **out) {
 }
 
 static void dev_free(mb_dev *d) {
-    cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso); cudaFree(d->trip); cudaFree(d->tboff);
+    cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso); cudaFree(d->trip); cudaFree(d->tboff); cudaFree(d->lhash);
     cudaFree(d->X); cudaFree(d->V); cudaFree(d->spc); cudaFree(d->nn); cudaFree(d->nj); cudaFree(d->nd);
     cudaFree(d->F); cudaFree(d->EA); cudaFree(d->EU); cudaFree(d->vir); cudaFree(d->G);
     cudaFree(d->cell_of); cudaFree(d->cell_cnt); cudaFree(d->cell_start); cudaFree(d->cell_atoms);
@@ -410,16 +410,17 @@ static int ensure(mb_potential *p, int N, int nb, int ncell) {
         d->capN = cap;
         p->gen++;
         cudaFree(d->nj); cudaFree(d->nd); cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso);
-        cudaFree(d->trip); cudaFree(d->tboff);
+        cudaFree(d->trip); cudaFree(d->tboff); cudaFree(d->lhash);
         d->nj = NULL; d->nd = NULL; d->nk = NULL; d->leg = NULL; d->nso = NULL; d->trip = NULL; d->tboff = NULL;
+        d->lhash = NULL;
         d->capNB = 0;
     }
     if (nb > d->capNB || !d->nj) {
         int cap = nb > d->capNB ? nb : d->capNB;
         cap = (cap + 7) & ~7;
         cudaFree(d->nj); cudaFree(d->nd); cudaFree(d->nk); cudaFree(d->leg); cudaFree(d->nso);
-        cudaFree(d->trip); cudaFree(d->tboff);
-        d->nk = NULL; d->leg = NULL; d->nso = NULL; d->trip = NULL; d->tboff = NULL;
+        cudaFree(d->trip); cudaFree(d->tboff); cudaFree(d->lhash);
+        d->nk = NULL; d->leg = NULL; d->nso = NULL; d->trip = NULL; d->tboff = NULL; d->lhash = NULL;
         CK(cudaMalloc((void **)&d->nj, sizeof(int) * (size_t)cap * d->capN), "alloc nj");
         CK(cudaMalloc((void **)&d->nd, sizeof(double) * 4 * (size_t)cap * d->capN), "alloc nd");
         if (p->legs_enabled && cap <= MB_LEG_MAX_CAP) {
@@ -430,6 +431,7 @@ static int ensure(mb_potential *p, int N, int nb, int ncell) {
             d->tcap = cap * (cap - 1) / 2;
             CK(cudaMalloc((void **)&d->trip, 2 * sizeof(unsigned) * (size_t)d->tcap * d->capN), "alloc trip");
             CK(cudaMalloc((void **)&d->tboff, sizeof(int) * 8 * (size_t)d->capN), "alloc tboff");
+            CK(cudaMalloc((void **)&d->lhash, 2 * sizeof(unsigned) * 256 * (size_t)d->capN), "alloc list hash");
         }
         d->capNB = cap;
         p->gen++;

@@ -22,6 +22,16 @@
 /* atomic masses (amu) by atomic number and minimum interatomic distances
  * (Angstrom) used by the short-range repulsion; physical data tables that
  * must agree with the reference (src/util.c:11,13). */
+/* the smallest double t with sqrt(t) >= R (R > 0): s < t exactly when
+ * sqrt(s) < R, since sqrt is correctly rounded and non-decreasing */
+static double sqrt_threshold(double R) {
+    double t = R * R;
+    if (!(R > 0.0)) return 0.0;
+    while (sqrt(t) < R) t = nextafter(t, INFINITY);
+    while (t > 0.0 && sqrt(nextafter(t, 0.0)) >= R) t = nextafter(t, 0.0);
+    return t;
+}
+
 static const double mb_atom_mass[96] = {
     0.0, 1.008, 4.002602, 6.94, 9.0121831, 10.81, 12.011, 14.007, 15.999, 18.99840316, 20.1797, 22.98976928,
     24.305, 26.9815384, 28.085, 30.973762, 32.06, 35.45, 39.948, 39.0983, 40.078, 44.955908, 47.867, 50.9415,
@@ -260,6 +270,7 @@ static int parse_basis(const mb_lines *L, mb_model *m, char *err, size_t el) {
                 P->f_rc2[p] = W->gp[0][gf[0][1]];
                 P->f_rc4[p] = P->ng4 ? W->gp[0][gf[g4first][1]] : 0.0;
                 P->f_rc4sq[p] = P->f_rc4[p] * P->f_rc4[p];
+                P->f_rc4thr[p] = sqrt_threshold(P->f_rc4[p]);
                 for (f = 0; f < P->ng2; f++) {
                     P->f_eta2[p][f] = W->gp[2][gf[f][3]];
                     P->f_rs[p][f] = W->gp[1][gf[f][2]];

@@ -31,6 +31,10 @@ typedef struct {
     int ind2[4], ind4[20];
     /* forward parameters per pair index p = s0*s0+s1*s1 */
     double f_rc2[MB_NPAIR], f_rc4[MB_NPAIR], f_rc4sq[MB_NPAIR];
+    /* the smallest double t with sqrt(t) >= f_rc4: s < t exactly when
+     * sqrt(s) < f_rc4, the reference's test of a triplet's j-k distance
+     * (src/nprs.c:536) without a square root */
+    double f_rc4thr[MB_NPAIR];
     double f_eta2[MB_NPAIR][MB_MAXG2], f_rs[MB_NPAIR][MB_MAXG2];
     double f_eta4[MB_NPAIR][MB_MAXE];
     /* derivative parameters (species-0 block) */
@@ -144,6 +148,7 @@ typedef struct {
     void *trip;
     int *tboff;
     int tcap;
+    void *lhash;      /* [N*256] uint2 (key, slot) per atom: the hash of its list (k_legs) */
     int legs_on;
     /* optional CUDA-event timing of the descriptor kernel */
     int ev_on, ev_n, ev_cap;

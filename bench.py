@@ -39,8 +39,8 @@ METRIC = "atom-steps/s (E+F+stress) & relaxed structures/s vs plain GPU path"
 UNIT = "atom-steps/s"
 WORKLOAD = "CuPdAg fcc 10x10x10 (4000 atoms), 282-10-10-1 FP64, Rc 6 A, NVT 600 K, dt 1 fs"
 SETTLE_STEPS = 20  # untimed NVT steps from the ideal lattice before the warm-up
-KERNEL_NAME = ("descriptor pass: k_legs (leg tables) + k_efs_leg (fused descriptors + MLP + forces + virial), "
-               "timed together")
+KERNEL_NAME = ("descriptor pass: k_legs (leg tables) + k_trip (triplet lists) + k_efs_leg (fused descriptors + "
+               "MLP + forces + virial), timed together")
 KERNEL_NAME_NOLEGS = "descriptor pass: k_efs (fused descriptors + MLP + forces + virial)"
 
 
@@ -152,11 +152,12 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_efs_md4000.md")
+    """DRAM bytes of one descriptor pass (k_legs + k_trip + k_efs_leg, one
+    ncu capture each) from the committed summary."""
+    path = os.path.join(ROOT, "profiles", "descriptor_pass_md4000.md")
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith("traffic_bytes_per_pass:"):
                 return float(line.split(":")[1])
     except Exception:
         pass

@@ -1223,11 +1223,13 @@ __device__ __forceinline__ unsigned hash_slot(unsigned key) { return (key * 0x9E
 __global__ void k_legs(int N, int cap, const int *__restrict__ nn, int *__restrict__ nj, unsigned *__restrict__ nk,
                        double4 *__restrict__ nd, const int *__restrict__ spc, const mb_params *__restrict__ Pg,
                        double *__restrict__ leg, int *__restrict__ nso, uint2 *__restrict__ gh) {
+    /* the hash is built in shared memory, then copied out whole */
+    __shared__ uint2 hsh[4][LEG_HASH];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= N) return;
     const int i = warp, n = nn[i], s0 = spc[i], ne = Pg->ne;
     const size_t row = (size_t)i * cap;
-    uint2 *hash = gh + (size_t)i * LEG_HASH;
+    uint2 *hash = hsh[(threadIdx.x >> 5) & 3];
     for (int t = lane; t < LEG_HASH; t += 32) hash[t] = make_uint2(0xffffffffu, 0u);
     int jv[LEG_PER_LANE], spv[LEG_PER_LANE];
     unsigned kv[LEG_PER_LANE];
@@ -1294,6 +1296,9 @@ __global__ void k_legs(int N, int cap, const int *__restrict__ nn, int *__restri
             for (int k = 0; k < MB_LEG_STRIDE / 2; k++) o[k] = make_double2(e[2 * k], e[2 * k + 1]);
         }
     }
+    __syncwarp();
+    uint2 *out = gh + (size_t)i * LEG_HASH;
+    for (int t = lane; t < LEG_HASH; t += 32) out[t] = hash[t];
 }
 
 struct LegArgs {
@@ -1574,13 +1579,16 @@ __device__ __forceinline__ void leg_run_conv(const LegSmem &s, const uint2 *__re
  * read from the rows k_legs wrote (i-j and i-k from i's own rows, staged;
  * j-k from j's row in global memory, L2-resident).  Reference bases: at
  * most 8 G4 exponents, zeta in {1, 2, 4, 16} or other integers, 2 lambdas. */
-/* every shape is compiled for 12 resident warps per SM (at most 170
- * registers a thread), the occupancy its shared memory also allows at the
- * alloy's neighbour counts.  RV selects the reverse pass's layout: 0 per-lane
- * runs of entries (a-side forces in registers), 1 consecutive entries per
- * round (b-side atomics without conflicts within a row). */
+/* Register budget per shape: the multi-warp shapes are compiled for 16
+ * resident warps per SM (at most 128 registers a thread; a few bytes of
+ * spills, measured 3-9% faster than 12 warps), the one-warp shapes for 12
+ * (their shared memory allows no more at the alloy's neighbour counts).
+ * RV selects the reverse pass's layout: 0 per-lane runs of entries (a-side
+ * forces in registers), 1 consecutive entries per round (b-side atomics
+ * without conflicts within a row). */
 template <int NE, int WPA, int APB, int RV>
-__global__ void __launch_bounds__(WPA * 32 * APB, 384 / (WPA * 32 * APB)) k_efs_leg(const __grid_constant__ LegArgs A) {
+__global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA * 32 * APB))
+    k_efs_leg(const __grid_constant__ LegArgs A) {
     constexpr int NZ = 4, NLAM = 2, NZL = 8;
     static_assert(NE == 7 || NE == 8, "leg rows hold 8 exponents");
     extern __shared__ __align__(16) char smem_raw[];

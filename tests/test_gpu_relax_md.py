@@ -121,11 +121,15 @@ def test_md_results_independent_of_chunking(mb, tmp_path):
 
 
 @pytest.mark.parametrize("size", [2, 5])
-def test_md_graph_replay_equals_plain_launches(mb, tmp_path, size):
+def test_md_graph_replay_equals_plain_launches(mb, tmp_path, size, monkeypatch):
     """The NVT loop replayed as captured CUDA graphs (chunks of 10 steps, a
     shorter last chunk, a second call reusing the graph) gives the trajectory
-    of plain launches; 32 atoms take the all-pairs list, 500 the cell list."""
+    of plain launches; 32 atoms take the all-pairs list, 500 the cell list.
+    Both handles run one fixed kernel variant, so that their launch counts
+    compare (each handle's autotuner could otherwise pick another family)."""
     from maise_b200 import atomic_mass, maxwell, models, workloads
+
+    monkeypatch.setenv("MAISE_B200_SHAPE", "6")
 
     w = workloads.random_alloy(n=size, a=3.8, seed=9, species=(29, 46), jitter=0.05)
     d = tmp_path / "m"

@@ -238,60 +238,88 @@ __global__ void k_cell_sort(int ncell, const int *start, int *atoms) {
 /* One warp per atom over the 27 adjacent cells.  Periodic directions have
  * at least 3 bins no thinner than Rc, so every image within Rc lies in an
  * adjacent bin and each (atom, image) pair is visited once; the exact test
- * then selects the reference's set. */
+ * then selects the reference's set.  The 27 cells' atom ranges are laid end
+ * to end (cell order a, b, e; atoms in index order within a cell) and
+ * walked 32 candidates per round, every lane busy. */
 __global__ void k_nlist_cell(int N, int NM, int cap, const double *__restrict__ X, mb_cell c, double rc2,
                              const int *__restrict__ cell_of, const int *__restrict__ start,
                              const int *__restrict__ atoms, int *__restrict__ nn, int *__restrict__ nj,
                              double4 *__restrict__ nd, int *status, unsigned *__restrict__ nk) {
+    __shared__ int s_off[4][32], s_lo[4][32], s_img[4][32];
+    const int w = (threadIdx.x >> 5) & 3;
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= N) return;
     int i = warp;
     double xi[3] = {X[3 * i], X[3 * i + 1], X[3 * i + 2]};
     int ci = cell_of[i];
     int cq[3] = {ci / (c.M[1] * c.M[2]), (ci / c.M[2]) % c.M[1], ci % c.M[2]};
-    int count = 0;
-    for (int a = -1; a <= 1; a++)
-        for (int b = -1; b <= 1; b++)
-            for (int e = -1; e <= 1; e++) {
-                int dd[3] = {a, b, e}, cc[3], img[3];
-                bool skip = false;
-                for (int q = 0; q < 3; q++) {
-                    int k = cq[q] + dd[q];
-                    img[q] = 0;
-                    if (q < c.ND) {
-                        if (k < 0) { k += c.M[q]; img[q] = -1; }
-                        else if (k >= c.M[q]) { k -= c.M[q]; img[q] = 1; }
-                    } else if (k < 0 || k >= c.M[q]) {
-                        skip = true;
-                    }
-                    cc[q] = k;
-                }
-                if (skip) continue;
-                int cell = (cc[0] * c.M[1] + cc[1]) * c.M[2] + cc[2];
-                int lo = start[cell], hi = start[cell + 1];
-                for (int base = lo; base < hi; base += 32) {
-                    int idx = base + lane;
-                    bool ok = false;
-                    int j = 0;
-                    double d[3] = {0, 0, 0}, r2 = 0.0;
-                    if (idx < hi) {
-                        j = atoms[idx];
-                        if (!(j == i && img[0] == 0 && img[1] == 0 && img[2] == 0)) {
-                            double xj[3] = {X[3 * j], X[3 * j + 1], X[3 * j + 2]};
-                            r2 = image_disp(c, xi, xj, img[0], img[1], img[2], d);
-                            ok = r2 < rc2;
-                        }
-                    }
-                    unsigned m = __ballot_sync(FULL, ok);
-                    int pos = count + __popc(m & ((1u << lane) - 1u));
-                    if (ok && pos < cap) {
-                        nj[(size_t)i * cap + pos] = j;
-                        nd[(size_t)i * cap + pos] = make_double4(d[0], d[1], d[2], sqrt(r2));
-                        if (nk) nk[(size_t)i * cap + pos] = entry_key(j, img[0], img[1], img[2]);
-                    }
-                    count += __popc(m);
-                }
+    /* lane k < 27 describes adjacent cell k = 9 (a+1) + 3 (b+1) + (e+1) */
+    int lo = 0, cnt = 0, pimg = 0;
+    if (lane < 27) {
+        const int dd[3] = {lane / 9 - 1, (lane / 3) % 3 - 1, lane % 3 - 1};
+        int cc[3], img[3];
+        bool skip = false;
+        for (int q = 0; q < 3; q++) {
+            int k = cq[q] + dd[q];
+            img[q] = 0;
+            if (q < c.ND) {
+                if (k < 0) { k += c.M[q]; img[q] = -1; }
+                else if (k >= c.M[q]) { k -= c.M[q]; img[q] = 1; }
+            } else if (k < 0 || k >= c.M[q]) {
+                skip = true;
             }
+            cc[q] = k;
+        }
+        if (!skip) {
+            const int cell = (cc[0] * c.M[1] + cc[1]) * c.M[2] + cc[2];
+            lo = start[cell];
+            cnt = start[cell + 1] - lo;
+        }
+        pimg = (img[0] + 1) * 9 + (img[1] + 1) * 3 + (img[2] + 1);
+    }
+    int off = cnt; /* inclusive scan of the cell sizes */
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, off, o);
+        if (lane >= o) off += y;
+    }
+    const int total = __shfl_sync(FULL, off, 31);
+    s_off[w][lane] = off - cnt; /* exclusive */
+    s_lo[w][lane] = lo;
+    s_img[w][lane] = pimg;
+    __syncwarp();
+    int count = 0;
+    for (int base = 0; base < total; base += 32) {
+        const int t = base + lane;
+        bool ok = false;
+        int j = 0, img[3] = {0, 0, 0};
+        double d[3] = {0, 0, 0}, r2 = 0.0;
+        if (t < total) {
+            /* the last of the 27 cells whose range starts at or before t */
+            int k = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+                if (k + step < 27 && s_off[w][k + step] <= t) k += step;
+            j = atoms[s_lo[w][k] + (t - s_off[w][k])];
+            const int pi = s_img[w][k];
+            img[0] = pi / 9 - 1;
+            img[1] = (pi / 3) % 3 - 1;
+            img[2] = pi % 3 - 1;
+            if (!(j == i && img[0] == 0 && img[1] == 0 && img[2] == 0)) {
+                double xj[3] = {X[3 * j], X[3 * j + 1], X[3 * j + 2]};
+                r2 = image_disp(c, xi, xj, img[0], img[1], img[2], d);
+                ok = r2 < rc2;
+            }
+        }
+        unsigned m = __ballot_sync(FULL, ok);
+        int pos = count + __popc(m & ((1u << lane) - 1u));
+        if (ok && pos < cap) {
+            nj[(size_t)i * cap + pos] = j;
+            nd[(size_t)i * cap + pos] = make_double4(d[0], d[1], d[2], sqrt(r2));
+            if (nk) nk[(size_t)i * cap + pos] = entry_key(j, img[0], img[1], img[2]);
+        }
+        count += __popc(m);
+    }
     if (lane == 0) {
         nn[i] = count < cap ? count : cap;
         if (count >= NM) atomicOr(status, MB_ST_NBR_OVERFLOW);
@@ -2253,7 +2281,7 @@ extern "C" int mbk_nlist(mb_dev *d, int N, int NM, const mb_cell *c, double rc, 
         k_cell_scan<<<1, 1024, 0, st>>>(ncell, d->cell_cnt, d->cell_start);
         cudaMemsetAsync(d->cell_cnt, 0, sizeof(int) * ncell, st);
         k_cell_fill<<<(N + 127) / 128, 128, 0, st>>>(N, d->cell_of, d->cell_start, d->cell_cnt, d->cell_atoms);
-        k_cell_sort<<<(ncell + 127) / 128, 128, 0, st>>>(ncell, d->cell_start, d->cell_atoms);
+        k_cell_sort<<<(ncell + 3) / 4, 128, 0, st>>>(ncell, d->cell_start, d->cell_atoms); /* a warp per cell */
         k_nlist_cell<<<blocks, warps_per_block * 32, 0, st>>>(N, NM, d->capNB, d->X, *c, rc2, d->cell_of,
                                                               d->cell_start, d->cell_atoms, d->nn, d->nj,
                                                               (double4 *)d->nd, d->status,

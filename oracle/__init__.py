@@ -41,7 +41,9 @@ def _ip(a):
 
 # Where the build recipe looks for the reference MAISE sources: the
 # MAISE_REFERENCE environment variable, else the read-only mount point of the
-# build container.  Nothing at test or benchmark time reads the sources.
+# build container.  Besides the build, only CPU tests that pin the oracle to
+# the reference's own fixture files read it (and skip without it); nothing
+# in the GPU tests, smoke() or the benchmark does.
 _REFERENCE_MOUNT = "/root/reference"
 
 

@@ -111,7 +111,7 @@ struct BShared {
     double uvir[6];
     double red[W * 32];
     double scal[24];
-    float F[BMAXN * 3];
+    double F[BMAXN * 3];
     int spc[BMAXN];
     int nn[BMAXN];
     int s, N, ndof, flag, cmd, first;
@@ -540,6 +540,10 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
 
     /* reverse pairs (species-0 derivative parameters) */
     float fi0 = 0.0f, fi1 = 0.0f, fi2 = 0.0f;
+    /* the repulsion's force on atom i, kept in FP64 to the structure's
+     * force array: at short distances it is the largest term (hundreds of
+     * eV/A) and an FP32 sum of it would carry most of the rounding */
+    double fu0 = 0.0, fu1 = 0.0, fu2 = 0.0;
     double vr[6] = {0, 0, 0, 0, 0, 0};
     for (int t = lane; t < n; t += 32) {
         float4 d = ws.d[t];
@@ -569,7 +573,7 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
                 sincospi(rd / R, &sn, &cs);
                 double fu = 0.5 * (1.0 + cs), dfu = -0.5 * CUDART_PI / R * sn;
                 double tu = -2.0 * A.urep * R / (rd * rd) * (-fu / rd + dfu);
-                fi0 -= (float)(tu * d.x); fi1 -= (float)(tu * d.y); fi2 -= (float)(tu * d.z);
+                fu0 -= tu * d.x; fu1 -= tu * d.y; fu2 -= tu * d.z;
                 vr[0] += 0.5 * tu * d.x * d.x; vr[1] += 0.5 * tu * d.y * d.y; vr[2] += 0.5 * tu * d.z * d.z;
                 vr[3] += 0.5 * tu * d.x * d.y; vr[4] += 0.5 * tu * d.y * d.z; vr[5] += 0.5 * tu * d.z * d.x;
             }
@@ -615,86 +619,88 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
                     __syncwarp();
                 }
                 {
-                    /* each lane takes a contiguous run of K list entries (K odd, so
-                     * that the lanes' reads of the list fall in distinct banks); the
-                     * list runs row by row, so a lane's entries mostly share j and
-                     * the j-side force is summed in registers and written once per
-                     * change of j */
-                    int K = (hi - lo + 31) >> 5;
-                    if (K > 0) K |= 1;
-                    const int t0 = lo + lane * K;
-                    int cj = -1;
-                    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-                    for (int step = 0; step < K; step++) {
-                        const int t = t0 + step;
-                        if (t >= hi) break;
-                        const unsigned pk = ws.tl[t];
-                        const int jj = pk & 0xffff, kk = pk >> 16;
-                        const float4 d1 = ws.d[jj], d2 = ws.d[kk];
+                    /* 32 consecutive list entries per round: the list runs row by
+                     * row, so within a round the lanes of one row j are contiguous
+                     * and their k differ (the k-side atomics rarely collide); the
+                     * j-side forces are summed per row by a segmented warp sum and
+                     * added by the row's first lane */
+                    for (int base = lo; base < hi; base += 32) {
+                        const int t = base + lane;
+                        int jj = -1 - lane, kk = 0;
+                        float g1x = 0.0f, g1y = 0.0f, g1z = 0.0f;
+                        if (t < hi) {
+                            const unsigned pk = ws.tl[t];
+                            jj = pk & 0xffff;
+                            kk = pk >> 16;
+                        }
+                        const float4 d1 = ws.d[max(jj, 0)], d2 = ws.d[kk];
                         const float wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
                         const float r3s = wx * wx + wy * wy + wz * wz, r3 = sqrtf(r3s);
-                        if (!(d1.w < drc4 && d2.w < drc4 && r3s < drc4sq)) continue;
-                        float r1 = d1.w, r2 = d2.w, ir1 = ws.ir[jj], ir2 = ws.ir[kk], ir3 = 1.0f / r3;
-                        float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
-                        float f3, df3;
-                        fcutf_d(drc4, r3, f3, df3);
-                        float f1 = ws.fa[jj], df1 = ws.fb[jj], f2 = ws.fa[kk], df2 = ws.fb[kk];
-                        float lz[BNZL], lzp[BNZL];
-                        angularf(P, c, lz, lzp);
-                        float Q = 0.0f, Qe = 0.0f, Qc = 0.0f;
-                        const float4 *pj = reinterpret_cast<const float4 *>(ws.P + jj * 8);
-                        const float4 *pk4 = reinterpret_cast<const float4 *>(ws.P + kk * 8);
-                        const float4 ja = pj[0], jb = pj[1], ka = pk4[0], kb4 = pk4[1];
-                        const float pjk[8] = {ja.x * ka.x, ja.y * ka.y, ja.z * ka.z, ja.w * ka.w,
-                                              jb.x * kb4.x, jb.y * kb4.y, jb.z * kb4.z, jb.w * kb4.w};
-                        const float4 *g4 = reinterpret_cast<const float4 *>(ws.grid);
+                        if (t < hi && d1.w < drc4 && d2.w < drc4 && r3s < drc4sq) {
+                            float r1 = d1.w, r2 = d2.w, ir1 = ws.ir[jj], ir2 = ws.ir[kk], ir3 = 1.0f / r3;
+                            float c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
+                            float f3, df3;
+                            fcutf_d(drc4, r3, f3, df3);
+                            float f1 = ws.fa[jj], df1 = ws.fb[jj], f2 = ws.fa[kk], df2 = ws.fb[kk];
+                            float lz[BNZL], lzp[BNZL];
+                            angularf(P, c, lz, lzp);
+                            float Q = 0.0f, Qe = 0.0f, Qc = 0.0f;
+                            const float4 *pj = reinterpret_cast<const float4 *>(ws.P + jj * 8);
+                            const float4 *pk4 = reinterpret_cast<const float4 *>(ws.P + kk * 8);
+                            const float4 ja = pj[0], jb = pj[1], ka = pk4[0], kb4 = pk4[1];
+                            const float pjk[8] = {ja.x * ka.x, ja.y * ka.y, ja.z * ka.z, ja.w * ka.w,
+                                                  jb.x * kb4.x, jb.y * kb4.y, jb.z * kb4.z, jb.w * kb4.w};
+                            const float4 *g4 = reinterpret_cast<const float4 *>(ws.grid);
 #pragma unroll
-                        for (int q = 0; q < BNE; q++) {
-                            const float ex = pjk[q] * expf(-deta[q] * r3s);
-                            const float4 ga = g4[2 * q], gb = g4[2 * q + 1];
-                            const float cg[8] = {ga.x, ga.y, ga.z, ga.w, gb.x, gb.y, gb.z, gb.w};
-                            /* (u, v) = sum over cells of cg * (lz, lz') with paired FMAs */
-                            float2 uv = make_float2(0.0f, 0.0f);
+                            for (int q = 0; q < BNE; q++) {
+                                const float ex = pjk[q] * expf(-deta[q] * r3s);
+                                const float4 ga = g4[2 * q], gb = g4[2 * q + 1];
+                                const float cg[8] = {ga.x, ga.y, ga.z, ga.w, gb.x, gb.y, gb.z, gb.w};
+                                /* (u, v) = sum over cells of cg * (lz, lz') with paired FMAs */
+                                float2 uv = make_float2(0.0f, 0.0f);
 #pragma unroll
-                            for (int zl = 0; zl < BNZL; zl++)
-                                uv = __ffma2_rn(make_float2(cg[zl], cg[zl]), make_float2(lz[zl], lzp[zl]), uv);
-                            const float u = uv.x, vv = uv.y;
-                            Q += ex * u;
-                            Qe += deta[q] * ex * u;
-                            Qc += ex * vv;
-                        }
-                        float Af = 2.0f * f1 * f2 * f3;
-                        float T1 = 2.0f * df1 * f2 * f3 * Q - 2.0f * r1 * Af * Qe;
-                        float T2 = 2.0f * f1 * df2 * f3 * Q - 2.0f * r2 * Af * Qe;
-                        float T3 = 2.0f * f1 * f2 * df3 * Q - 2.0f * r3 * Af * Qe;
-                        float Tc = Af * Qc;
-                        float a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
-                        float a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
-                        const float g1x = a11 * d1.x + a12 * d2.x - a3 * wx;
-                        const float g1y = a11 * d1.y + a12 * d2.y - a3 * wy;
-                        const float g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
-                        const float g2x = a22 * d2.x + a12 * d1.x + a3 * wx;
-                        const float g2y = a22 * d2.y + a12 * d1.y + a3 * wy;
-                        const float g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
-                        fi0 += g1x + g2x; fi1 += g1y + g2y; fi2 += g1z + g2z;
-                        atomicAdd(&ws.Fnb[3 * kk], -g2x);
-                        atomicAdd(&ws.Fnb[3 * kk + 1], -g2y);
-                        atomicAdd(&ws.Fnb[3 * kk + 2], -g2z);
-                        if (jj != cj) {
-                            if (cj >= 0) {
-                                atomicAdd(&ws.Fnb[3 * cj], -sx);
-                                atomicAdd(&ws.Fnb[3 * cj + 1], -sy);
-                                atomicAdd(&ws.Fnb[3 * cj + 2], -sz);
+                                for (int zl = 0; zl < BNZL; zl++)
+                                    uv = __ffma2_rn(make_float2(cg[zl], cg[zl]), make_float2(lz[zl], lzp[zl]), uv);
+                                const float u = uv.x, vv = uv.y;
+                                Q += ex * u;
+                                Qe += deta[q] * ex * u;
+                                Qc += ex * vv;
                             }
-                            cj = jj;
-                            sx = sy = sz = 0.0f;
+                            float Af = 2.0f * f1 * f2 * f3;
+                            float T1 = 2.0f * df1 * f2 * f3 * Q - 2.0f * r1 * Af * Qe;
+                            float T2 = 2.0f * f1 * df2 * f3 * Q - 2.0f * r2 * Af * Qe;
+                            float T3 = 2.0f * f1 * f2 * df3 * Q - 2.0f * r3 * Af * Qe;
+                            float Tc = Af * Qc;
+                            float a11 = T1 * ir1 - Tc * c * ir1 * ir1, a22 = T2 * ir2 - Tc * c * ir2 * ir2;
+                            float a12 = Tc * ir1 * ir2, a3 = T3 * ir3;
+                            g1x = a11 * d1.x + a12 * d2.x - a3 * wx;
+                            g1y = a11 * d1.y + a12 * d2.y - a3 * wy;
+                            g1z = a11 * d1.z + a12 * d2.z - a3 * wz;
+                            const float g2x = a22 * d2.x + a12 * d1.x + a3 * wx;
+                            const float g2y = a22 * d2.y + a12 * d1.y + a3 * wy;
+                            const float g2z = a22 * d2.z + a12 * d1.z + a3 * wz;
+                            fi0 += g1x + g2x; fi1 += g1y + g2y; fi2 += g1z + g2z;
+                            atomicAdd(&ws.Fnb[3 * kk], -g2x);
+                            atomicAdd(&ws.Fnb[3 * kk + 1], -g2y);
+                            atomicAdd(&ws.Fnb[3 * kk + 2], -g2z);
                         }
-                        sx += g1x; sy += g1y; sz += g1z;
-                    }
-                    if (cj >= 0) {
-                        atomicAdd(&ws.Fnb[3 * cj], -sx);
-                        atomicAdd(&ws.Fnb[3 * cj + 1], -sy);
-                        atomicAdd(&ws.Fnb[3 * cj + 2], -sz);
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const float x = __shfl_down_sync(FULLM, g1x, o), y = __shfl_down_sync(FULLM, g1y, o),
+                                        z = __shfl_down_sync(FULLM, g1z, o);
+                            const int jn = __shfl_down_sync(FULLM, jj, o);
+                            if (lane + o < 32 && jn == jj) {
+                                g1x += x;
+                                g1y += y;
+                                g1z += z;
+                            }
+                        }
+                        const int jp = __shfl_up_sync(FULLM, jj, 1);
+                        if (jj >= 0 && (lane == 0 || jp != jj)) {
+                            atomicAdd(&ws.Fnb[3 * jj], -g1x);
+                            atomicAdd(&ws.Fnb[3 * jj + 1], -g1y);
+                            atomicAdd(&ws.Fnb[3 * jj + 2], -g1z);
+                        }
                     }
                 }
                 __syncwarp();
@@ -711,19 +717,19 @@ __device__ void atom_pass(const BArgs &A, BShared<W> &sh, WarpWS &ws, int i, con
         vr[3] += fx * d.y; vr[4] += fy * d.z; vr[5] += fz * d.x;
     }
     /* gather: atom i and its neighbours into the structure's force array */
-    fi0 = bsumf(fi0);
-    fi1 = bsumf(fi1);
-    fi2 = bsumf(fi2);
-    if (lane == 0) {
-        atomicAdd(&sh.F[3 * i], fi0);
-        atomicAdd(&sh.F[3 * i + 1], fi1);
-        atomicAdd(&sh.F[3 * i + 2], fi2);
+    {
+        const double s0x = bsum((double)fi0 + fu0), s0y = bsum((double)fi1 + fu1), s0z = bsum((double)fi2 + fu2);
+        if (lane == 0) {
+            atomicAdd(&sh.F[3 * i], s0x);
+            atomicAdd(&sh.F[3 * i + 1], s0y);
+            atomicAdd(&sh.F[3 * i + 2], s0z);
+        }
     }
     for (int t = lane; t < n; t += 32) {
         int j = ws.j[t];
-        atomicAdd(&sh.F[3 * j], ws.Fnb[3 * t]);
-        atomicAdd(&sh.F[3 * j + 1], ws.Fnb[3 * t + 1]);
-        atomicAdd(&sh.F[3 * j + 2], ws.Fnb[3 * t + 2]);
+        atomicAdd(&sh.F[3 * j], (double)ws.Fnb[3 * t]);
+        atomicAdd(&sh.F[3 * j + 1], (double)ws.Fnb[3 * t + 1]);
+        atomicAdd(&sh.F[3 * j + 2], (double)ws.Fnb[3 * t + 2]);
     }
 #pragma unroll
     for (int k = 0; k < 6; k++) virw[k] += bsum(vr[k]);
@@ -758,7 +764,7 @@ __device__ void eval_part(const BArgs &A, BShared<W> &sh, const double *dof, int
         double f[3];
         for (int q = 0; q < 3; q++) f[q] = dof[3 * a + q] - floor(dof[3 * a + q]);
         for (int q = 0; q < 3; q++) sh.xc[3 * a + q] = f[0] * sh.L[q] + f[1] * sh.L[3 + q] + f[2] * sh.L[6 + q];
-        sh.F[3 * a] = sh.F[3 * a + 1] = sh.F[3 * a + 2] = 0.0f;
+        sh.F[3 * a] = sh.F[3 * a + 1] = sh.F[3 * a + 2] = 0.0;
     }
     if (tid < 6) sh.uvir[tid] = 0.0;
     __syncthreads();
@@ -868,7 +874,7 @@ __device__ void eval_combine(BShared<W> &sh) {
             sh.eu[a] = ro->eu[a];
         }
         for (int q = 0; q < 3; q++) {
-            float f = sh.F[3 * a + q];
+            double f = sh.F[3 * a + q];
             for (int r = 1; r < C; r++) f += cl.map_shared_rank(&sh, r)->F[3 * a + q];
             sh.F[3 * a + q] = f;
         }
@@ -920,9 +926,9 @@ __device__ double eval_finish(const BArgs &A, BShared<W> &sh, double *gout) {
     for (int a = tid; a < N; a += blockDim.x)
         for (int q = 0; q < 3; q++) {
             double gq = 0.0;
-            for (int k = 0; k < 3; k++) gq -= (double)sh.F[3 * a + k] * sh.L[3 * q + k];
+            for (int k = 0; k < 3; k++) gq -= sh.F[3 * a + k] * sh.L[3 * q + k];
             gout[3 * a + q] = fabs(gq) < 1e-10 ? 0.0 : gq;
-            mf = fmax(mf, fabs((double)sh.F[3 * a + q]));
+            mf = fmax(mf, fabs(sh.F[3 * a + q]));
         }
     mf = cta_max(sh, mf);
     if (tid == 0) {
@@ -1265,7 +1271,7 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
          * evaluation was at the final DOF vector only if no step was taken */
         if (A.fout) {
             if (iter > 0) f = evaluate<W, C>(A, sh, sh.x, sh.g);
-            for (int k = tid; k < 3 * N; k += blockDim.x) A.fout[3 * (size_t)o + k] = (double)sh.F[k];
+            for (int k = tid; k < 3 * N; k += blockDim.x) A.fout[3 * (size_t)o + k] = sh.F[k];
             if (A.uout && tid < 6) A.uout[6 * (size_t)s + tid] = sh.uvir[tid] + (tid < 3 ? sh.scal[4] : 0.0);
             __syncthreads();
         }

@@ -172,3 +172,24 @@ def recall(pred, truth, keep_frac: float, top_frac: float = 0.10) -> float:
     ntop = max(1, int(round(top_frac * len(truth))))
     top = set(np.argsort(truth, kind="stable")[:ntop].tolist())
     return len(top & set(keep_best(pred, keep_frac).tolist())) / ntop
+
+
+def calibrate_keep(pred, truth, target: float = 0.99, top_frac: float = 0.10, margin: float = 0.02,
+                   step: float = 0.01) -> float:
+    """Keep fraction for a generation, chosen on held-out training pairs
+    (predictions `pred` of structures whose relaxed enthalpies `truth` are
+    known but were not fitted): the smallest fraction on a `step` grid from
+    `top_frac` up whose recall of the held-out best `top_frac` reaches
+    `target`, plus `margin`; 1.0 (relax everything) when no fraction below
+    1 does."""
+    pred, truth = np.asarray(pred), np.asarray(truth)
+    if len(pred) != len(truth) or len(pred) == 0:
+        raise ValueError("calibrate_keep: pred and truth must be non-empty and of one length")
+    k = 0
+    while True:
+        q = round(top_frac + k * step, 6)
+        if q >= 1.0:
+            return 1.0
+        if recall(pred, truth, q, top_frac) >= target:
+            return min(1.0, round(q + margin, 6))
+        k += 1

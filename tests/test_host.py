@@ -168,3 +168,22 @@ def test_chunked_population_does_not_depend_on_workers():
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x["X"], y["X"])
         np.testing.assert_array_equal(x["atmn"], y["atmn"])
+
+
+def test_keep_fraction_calibration_on_held_out_pairs():
+    from maise_b200.surrogate import calibrate_keep, recall
+
+    rng = np.random.default_rng(4)
+    truth = rng.normal(size=2000)
+    # a perfect screen needs no more than the best tenth, plus the margin
+    assert calibrate_keep(truth, truth, margin=0.02) == 0.12
+    # a noisy screen needs a wider keep, and the chosen keep reaches the target
+    pred = truth + rng.normal(scale=0.3, size=truth.size)
+    q = calibrate_keep(pred, truth, target=0.99, margin=0.0)
+    assert 0.12 < q < 1.0
+    assert recall(pred, truth, q) >= 0.99
+    assert recall(pred, truth, q - 0.01) < 0.99
+    # an anti-correlated screen finds nothing short of relaxing everything
+    assert calibrate_keep(-truth, truth) == 1.0
+    with pytest.raises(ValueError):
+        calibrate_keep([], [])

@@ -437,7 +437,16 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t
  * start on 16 bytes (the neighbour capacity is a multiple of 8) */
 __host__ __device__ constexpr int nep(int ne) { return (ne + 1) & ~1; }
 
-#define EFS_STG 17 /* staging row: 8 exponential + 8 angular values + 1 pad (banks) */
+#define EFS_STG 16 /* staging row: 8 exponential + 8 angular values */
+
+/* Staging slot of value q (0-7 exponential, 8-15 angular) of a warp's
+ * triplet t (0-31): rows of 16 doubles whose columns are rotated by
+ * 4 (t & 3) + ((t >> 2) & 3).  An 8-byte shared access is served a
+ * half-warp at a time; the writes (one q, 16 consecutive t) and the
+ * mma operand reads (4 consecutive t x 4 consecutive q) then both touch
+ * 16 distinct banks.  (A padded row of 17 left the operand reads 4-way
+ * conflicted.) */
+__device__ __forceinline__ int stg_slot(int t, int q) { return t * EFS_STG + ((q + 4 * (t & 3) + ((t >> 2) & 3)) & 15); }
 
 /* Sizes of the regions that share one block of memory: the forward
  * staging rows (tensor-core forward, live only while the forward triplets
@@ -931,17 +940,16 @@ __global__ void __launch_bounds__(WPA * 32 * APB, APB >= 4 ? 2 : 1) k_efs(EfsArg
                                 }
                             }
                         }
-                        double *row = stw + lane * EFS_STG;
 #pragma unroll
                         for (int q = 0; q < 8; q++) {
-                            row[q] = ex[q];
-                            row[8 + q] = lz[q];
+                            stw[stg_slot(lane, q)] = ex[q];
+                            stw[stg_slot(lane, 8 + q)] = lz[q];
                         }
                         __syncwarp();
 #pragma unroll
                         for (int st = 0; st < 8; st++) {
-                            const double *r = stw + (4 * st + (lane & 3)) * EFS_STG;
-                            dmma884(c0, c1, r[lane >> 2], r[8 + (lane >> 2)]);
+                            const int t = 4 * st + (lane & 3);
+                            dmma884(c0, c1, stw[stg_slot(t, lane >> 2)], stw[stg_slot(t, 8 + (lane >> 2))]);
                         }
                         __syncwarp();
                     };
@@ -1347,20 +1355,30 @@ struct LegArgs {
     mb_params P; /* by value: read from the kernel-parameter space through the constant cache */
 };
 
+/* Row of one list entry in k_efs_leg's shared memory: x, y, z, 1/r as two
+ * 16-byte loads, then r and a pad.  At 48 bytes a row, the 16-byte loads
+ * of 8 consecutive entries (a quarter-warp) fall in distinct banks; rows of
+ * 32 bytes (a double4) conflicted 2-way. */
+#define LEG_DROW 6
+__device__ __forceinline__ double4 leg_vec(const double *d, int u) {
+    const double2 *p = reinterpret_cast<const double2 *>(d + LEG_DROW * u);
+    const double2 a = p[0], b = p[1];
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
 /* shared-memory carve-up of one atom group of k_efs_leg */
 struct LegSmem {
     double *stage;                          /* tensor-core staging (forward) | */
     double *Fnb, *grid, *red, *h;           /* reductions, MLP, reverse pass   */
-    double4 *d;
-    double *ir, *L, *G;
+    double *d;                              /* per entry x, y, z, 1/r, r, 0    */
+    double *L, *G;
     double *tmp;                            /* G2 terms */
     int *j, *sp, *seg;
 };
 
 __host__ __device__ inline size_t leg_smem_bytes(int cap, int D, int ng2, int warps) {
     size_t b = efs_union_bytes(cap, 64, warps, 1);
-    b += sizeof(double4) * cap;
-    b += sizeof(double) * cap;                                 /* ir */
+    b += sizeof(double) * cap * LEG_DROW;                      /* d */
     b += sizeof(double) * cap * MB_LEG_STRIDE;                 /* L */
     b += align16(sizeof(double) * D);                          /* G */
     b += align16(sizeof(double) * cap * (ng2 > 1 ? ng2 : 1));  /* tmp */
@@ -1378,8 +1396,7 @@ __device__ inline LegSmem leg_carve(char *base, int cap, int D, int ng2, int war
     s.red = s.grid + 64;
     s.h = s.red + warps * 64;
     p += efs_union_bytes(cap, 64, warps, 1);
-    s.d = (double4 *)p; p += sizeof(double4) * cap;
-    s.ir = (double *)p; p += sizeof(double) * cap;
+    s.d = (double *)p; p += sizeof(double) * cap * LEG_DROW;
     s.L = (double *)p; p += sizeof(double) * cap * MB_LEG_STRIDE;
     s.G = (double *)p; p += align16(sizeof(double) * D);
     s.tmp = (double *)p; p += align16(sizeof(double) * cap * (ng2 > 1 ? ng2 : 1));
@@ -1664,8 +1681,10 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
         const double4 dv = A.nd[row + t];
         s.j[u] = j;
         s.sp[u] = sa;
-        s.d[u] = dv;
-        s.ir[u] = 1.0 / dv.w;
+        double2 *dr = reinterpret_cast<double2 *>(s.d + LEG_DROW * u);
+        dr[0] = make_double2(dv.x, dv.y);
+        dr[1] = make_double2(dv.z, 1.0 / dv.w);
+        dr[2] = make_double2(dv.w, 0.0);
         const double2 *src = reinterpret_cast<const double2 *>(A.leg + (row + t) * MB_LEG_STRIDE);
         double2 *dst = reinterpret_cast<double2 *>(s.L + (size_t)u * MB_LEG_STRIDE);
 #pragma unroll
@@ -1677,7 +1696,7 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
     if (A.mode != MB_MODE_VJP) {
         /* ---- forward pair terms: G2 (src/nprs.c:518-526) and repulsion ---- */
         for (int t = tid; t < n; t += NT) {
-            const double r = s.d[t].w;
+            const double r = s.d[LEG_DROW * t + 4];
             const int p = s0 * s0 + s.sp[t] * s.sp[t];
             const double fa = s.L[t * MB_LEG_STRIDE + 8]; /* one cutoff for all functions */
             for (int f = 0; f < ng2; f++) {
@@ -1695,7 +1714,7 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
         if (A.urep > 0.0 && tid == 0) {
             double eu = 0.0;
             for (int t = 0; t < n; t++) {
-                const double r = s.d[t].w, R = P.rm[s0] + P.rm[s.sp[t]];
+                const double r = s.d[LEG_DROW * t + 4], R = P.rm[s0] + P.rm[s.sp[t]];
                 if (r < R) eu += A.urep * fcut(R, r) * R / r;
             }
             A.EU[i] = eu;
@@ -1716,8 +1735,8 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
                     for (int q = 0; q < NZL; q++) lz[q] = 0.0;
                     if (valid) {
                         const int a = (int)(ent.x & 0xffu), b = (int)((ent.x >> 8) & 0xffu);
-                        const double4 d1 = s.d[a], d2 = s.d[b];
-                        const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (s.ir[a] * s.ir[b]);
+                        const double4 d1 = leg_vec(s.d, a), d2 = leg_vec(s.d, b);
+                        const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (d1.w * d2.w);
                         const double2 *la = reinterpret_cast<const double2 *>(s.L + a * MB_LEG_STRIDE);
                         const double2 *lb = reinterpret_cast<const double2 *>(s.L + b * MB_LEG_STRIDE);
                         const double2 *lg = reinterpret_cast<const double2 *>(A.leg + (size_t)ent.y * MB_LEG_STRIDE);
@@ -1730,17 +1749,16 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
                             if (2 * hh + 1 < NE) ex[2 * hh + 1] = A3 * (x.y * y.y) * z.y;
                         }
                     }
-                    double *rw = stw + lane * EFS_STG;
 #pragma unroll
                     for (int q = 0; q < 8; q++) {
-                        rw[q] = ex[q];
-                        rw[8 + q] = lz[q];
+                        stw[stg_slot(lane, q)] = ex[q];
+                        stw[stg_slot(lane, 8 + q)] = lz[q];
                     }
                     __syncwarp();
 #pragma unroll
                     for (int st = 0; st < 8; st++) {
-                        const double *r = stw + (4 * st + (lane & 3)) * EFS_STG;
-                        dmma884(c0, c1, r[lane >> 2], r[8 + (lane >> 2)]);
+                        const int t = 4 * st + (lane & 3);
+                        dmma884(c0, c1, stw[stg_slot(t, lane >> 2)], stw[stg_slot(t, 8 + (lane >> 2))]);
                     }
                     __syncwarp();
                 };
@@ -1819,8 +1837,8 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
     /* ---- reverse pair terms with the species-0 parameters ---- */
     double fi[3] = {0.0, 0.0, 0.0}, vr[6] = {0, 0, 0, 0, 0, 0};
     for (int t = tid; t < n; t += NT) {
-        const double4 d = s.d[t];
-        const double r = d.w, ir = s.ir[t];
+        const double4 d = leg_vec(s.d, t);
+        const double r = s.d[LEG_DROW * t + 4], ir = d.w;
         double f2, df2;
         fcut_d(P.d_rc2, r, f2, df2);
         const int ds1 = (s.sp[t] - s0 + ns) % ns;
@@ -1865,9 +1883,9 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
                 group_sync<WPA>();
                 auto body = [&](uint2 ent) -> double3 {
                     const int a = (int)(ent.x & 0xffu), b = (int)((ent.x >> 8) & 0xffu);
-                    const double4 d1 = s.d[a], d2 = s.d[b];
+                    const double4 d1 = leg_vec(s.d, a), d2 = leg_vec(s.d, b);
                     const double wx = d2.x - d1.x, wy = d2.y - d1.y, wz = d2.z - d1.z;
-                    const double ir1 = s.ir[a], ir2 = s.ir[b];
+                    const double ir1 = d1.w, ir2 = d2.w;
                     const double c = (d1.x * d2.x + d1.y * d2.y + d1.z * d2.z) * (ir1 * ir2);
                     const double2 *la = reinterpret_cast<const double2 *>(s.L + a * MB_LEG_STRIDE);
                     const double2 *lb = reinterpret_cast<const double2 *>(s.L + b * MB_LEG_STRIDE);
@@ -1933,7 +1951,7 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
 
     /* virial of atom i's energy: every neighbour force times its displacement */
     for (int t = tid; t < n; t += NT) {
-        const double4 d = s.d[t];
+        const double4 d = leg_vec(s.d, t);
         const double fx = s.Fnb[3 * t], fy = s.Fnb[3 * t + 1], fz = s.Fnb[3 * t + 2];
         vr[0] += fx * d.x; vr[1] += fy * d.y; vr[2] += fz * d.z;
         vr[3] += fx * d.y; vr[4] += fy * d.z; vr[5] += fz * d.x;

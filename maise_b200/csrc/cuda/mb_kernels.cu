@@ -1372,16 +1372,22 @@ struct LegSmem {
     double *Fnb, *grid, *red, *h;           /* reductions, MLP, reverse pass   */
     double *d;                              /* per entry x, y, z, 1/r, r, 0    */
     double *L, *G;
-    double *tmp;                            /* G2 terms */
+    double *tmp;                            /* G2 terms (in the stage region) */
     int *j, *sp, *seg;
 };
 
+/* The G2 terms (tmp) are read before the forward triplets start, so they
+ * share the region of the staging rows and the later reductions. */
+__host__ __device__ inline size_t leg_union_bytes(int cap, int ng2, int warps) {
+    const size_t u = efs_union_bytes(cap, 64, warps, 1), t = align16(sizeof(double) * cap * (ng2 > 1 ? ng2 : 1));
+    return u > t ? u : t;
+}
+
 __host__ __device__ inline size_t leg_smem_bytes(int cap, int D, int ng2, int warps) {
-    size_t b = efs_union_bytes(cap, 64, warps, 1);
+    size_t b = leg_union_bytes(cap, ng2, warps);
     b += sizeof(double) * cap * LEG_DROW;                      /* d */
     b += sizeof(double) * cap * MB_LEG_STRIDE;                 /* L */
     b += align16(sizeof(double) * D);                          /* G */
-    b += align16(sizeof(double) * cap * (ng2 > 1 ? ng2 : 1));  /* tmp */
     b += align16(sizeof(int) * cap) * 2;                       /* j, sp */
     b += sizeof(int) * 8;                                      /* seg */
     return align16(b);
@@ -1395,11 +1401,11 @@ __device__ inline LegSmem leg_carve(char *base, int cap, int D, int ng2, int war
     s.grid = s.Fnb + cap * 3;
     s.red = s.grid + 64;
     s.h = s.red + warps * 64;
-    p += efs_union_bytes(cap, 64, warps, 1);
+    s.tmp = (double *)p;
+    p += leg_union_bytes(cap, ng2, warps);
     s.d = (double *)p; p += sizeof(double) * cap * LEG_DROW;
     s.L = (double *)p; p += sizeof(double) * cap * MB_LEG_STRIDE;
     s.G = (double *)p; p += align16(sizeof(double) * D);
-    s.tmp = (double *)p; p += align16(sizeof(double) * cap * (ng2 > 1 ? ng2 : 1));
     s.j = (int *)p; p += align16(sizeof(int) * cap);
     s.sp = (int *)p; p += align16(sizeof(int) * cap);
     s.seg = (int *)p;
@@ -1490,52 +1496,81 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
             const bool tri = al == be;
             const int C = tri ? na * (na - 1) / 2 : na * nb;
             const float tb = (float)(2 * na - 1);
-            for (int base = 0; base < C; base += 32) {
-                const int c = base + lane;
-                bool ok = false;
-                uint2 ent = make_uint2(0u, 0u);
-                if (c < C) {
-                    int r, col;
-                    if (tri) {
-                        /* row r of the strict upper triangle starts at r (2 na - r - 1) / 2 */
-                        r = __float2int_rz(0.5f * (tb - sqrtf(fmaxf(tb * tb - 8.0f * (float)c, 0.0f))));
-                        r = min(max(r, 0), na - 2);
-                        while (r > 0 && r * (2 * na - r - 1) / 2 > c) r--;
-                        while (r < na - 2 && (r + 1) * (2 * na - r - 2) / 2 <= c) r++;
-                        col = c - r * (2 * na - r - 1) / 2 + r + 1;
-                    } else {
-                        r = c / nb;
-                        col = c - r * nb;
-                    }
-                    const int a = oa + r, b = ob + col;
-                    const double4 da = d[a], db = d[b];
-                    const double dx = xsub(da.x, db.x), dy = xsub(da.y, db.y), dz = xsub(da.z, db.z);
-                    const double s2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
-                    if (da.w < R01 && db.w < R02 && s2 < thr) {
-                        const unsigned ka = key[a], kb = key[b];
-                        const unsigned t = IMG_48 + spread_img(kb) - spread_img(ka);
-                        if ((t & IMG_BIT6) == 0u && (t & IMG_BIT5) == IMG_BIT5) {
-                            const unsigned f = (t & 31u) | ((t >> 2) & (31u << 5)) | ((t >> 4) & (31u << 10));
-                            const unsigned kk = (kb & ~0x7fffu) | (f ^ 0x4210u); /* k at its image relative to j */
-                            const int j = js[a];
-                            const uint2 *hj = gh + (size_t)j * LEG_HASH;
-                            unsigned h = hash_slot(kk);
-                            for (int probe = 0; probe < LEG_HASH; probe++) {
-                                const uint2 e = __ldg(hj + h);
-                                if (e.x == kk) {
-                                    ok = true;
-                                    ent = make_uint2((unsigned)a | ((unsigned)b << 8), (unsigned)j * (unsigned)cap + e.y);
-                                    break;
-                                }
-                                if (e.x == 0xffffffffu) break;
-                                h = (h + 1u) & (LEG_HASH - 1u);
+            /* two candidate pairs per lane and iteration (c and c + 32): both
+             * first hash probes are in flight together; entries are still
+             * written in candidate order */
+            for (int base = 0; base < C; base += 64) {
+                unsigned kk[2], h[2], ax[2], jx[2];
+                const uint2 *hj[2];
+                bool live[2];
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const int c = base + 32 * q + lane;
+                    live[q] = false;
+                    kk[q] = 0u;
+                    h[q] = 0u;
+                    ax[q] = 0u;
+                    jx[q] = 0u;
+                    hj[q] = gh;
+                    if (c < C) {
+                        int r, col;
+                        if (tri) {
+                            /* row r of the strict upper triangle starts at r (2 na - r - 1) / 2 */
+                            r = __float2int_rz(0.5f * (tb - sqrtf(fmaxf(tb * tb - 8.0f * (float)c, 0.0f))));
+                            r = min(max(r, 0), na - 2);
+                            while (r > 0 && r * (2 * na - r - 1) / 2 > c) r--;
+                            while (r < na - 2 && (r + 1) * (2 * na - r - 2) / 2 <= c) r++;
+                            col = c - r * (2 * na - r - 1) / 2 + r + 1;
+                        } else {
+                            r = c / nb;
+                            col = c - r * nb;
+                        }
+                        const int a = oa + r, b = ob + col;
+                        const double4 da = d[a], db = d[b];
+                        const double dx = xsub(da.x, db.x), dy = xsub(da.y, db.y), dz = xsub(da.z, db.z);
+                        const double s2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+                        if (da.w < R01 && db.w < R02 && s2 < thr) {
+                            const unsigned ka = key[a], kb = key[b];
+                            const unsigned t = IMG_48 + spread_img(kb) - spread_img(ka);
+                            if ((t & IMG_BIT6) == 0u && (t & IMG_BIT5) == IMG_BIT5) {
+                                const unsigned f = (t & 31u) | ((t >> 2) & (31u << 5)) | ((t >> 4) & (31u << 10));
+                                kk[q] = (kb & ~0x7fffu) | (f ^ 0x4210u); /* k at its image relative to j */
+                                const int j = js[a];
+                                jx[q] = (unsigned)j;
+                                hj[q] = gh + (size_t)j * LEG_HASH;
+                                h[q] = hash_slot(kk[q]);
+                                ax[q] = (unsigned)a | ((unsigned)b << 8);
+                                live[q] = true;
                             }
                         }
                     }
                 }
-                const unsigned m = __ballot_sync(FULL, ok);
-                if (ok) out[pos + __popc(m & ((1u << lane) - 1u))] = ent;
-                pos += __popc(m);
+                uint2 e[2];
+#pragma unroll
+                for (int q = 0; q < 2; q++) e[q] = live[q] ? __ldg(hj[q] + h[q]) : make_uint2(0xffffffffu, 0u);
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    bool ok = false;
+                    uint2 ent = make_uint2(0u, 0u);
+                    if (live[q]) {
+                        /* the first probe is in e[q]; at most LEG_HASH probes in all */
+                        uint2 x = e[q];
+                        unsigned hq = h[q];
+                        for (int probe = 0; probe < LEG_HASH; probe++) {
+                            if (x.x == kk[q]) {
+                                ok = true;
+                                ent = make_uint2(ax[q], jx[q] * (unsigned)cap + x.y);
+                                break;
+                            }
+                            if (x.x == 0xffffffffu) break;
+                            hq = (hq + 1u) & (LEG_HASH - 1u);
+                            x = __ldg(hj[q] + hq);
+                        }
+                    }
+                    const unsigned m = __ballot_sync(FULL, ok);
+                    if (ok) out[pos + __popc(m & ((1u << lane) - 1u))] = ent;
+                    pos += __popc(m);
+                }
             }
         }
     if (lane == 0) {

@@ -1430,7 +1430,11 @@ __device__ inline LegSmem leg_carve(char *base, int cap, int D, int ng2, int war
  * b), so every list is deterministic and at most cap (cap - 1) / 2 long;
  * tboff[8 i + blk] holds each block's start and tboff[8 i + nblk] the end.
  * counters[1] (if set) receives the number of triplets. */
-#define TRIP_WARPS 8
+/* 4 atoms per CTA: the CTAs all fit in one wave either way, and with
+ * smaller CTAs the SMs' shares of the 4000-atom alloy differ by 4 warps
+ * instead of 8 (about 7 us faster a pass than 8 atoms per CTA; 2 per CTA
+ * was no faster than 4) */
+#define TRIP_WARPS 4
 
 /* The 15-bit image field of an entry key (three 5-bit two's-complement
  * shifts) as three biased (x + 16) 7-bit fields, so that shifts add and

@@ -1111,10 +1111,12 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
         else if (maxf < A.fmax && maxu < A.fmax) status = 0;
         while (status == 1 && iter < A.mitr) {
             iter++;
-            /* p = -H g */
+            /* p = -H g; H is exactly symmetric (see the update below), so row r
+             * is read as column r: consecutive threads read consecutive
+             * elements */
             for (int r = tid; r < n; r += blockDim.x) {
                 double t = 0.0;
-                for (int c = 0; c < n; c++) t += H[r * n + c] * sh.g[c];
+                for (int c = 0; c < n; c++) t += H[c * n + r] * sh.g[c];
                 sh.p[r] = -t;
             }
             __syncthreads();
@@ -1245,7 +1247,7 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
                 /* Hy into g (g is replaced below) */
                 for (int r = tid; r < n; r += blockDim.x) {
                     double t = 0.0;
-                    for (int c = 0; c < n; c++) t += H[r * n + c] * sh.hy[c];
+                    for (int c = 0; c < n; c++) t += H[c * n + r] * sh.hy[c];
                     sh.g[r] = t;
                 }
                 __syncthreads();
@@ -1253,9 +1255,15 @@ __global__ void __launch_bounds__(W * 32) k_relax_batch(BArgs A) {
                 for (int k = tid; k < n; k += blockDim.x) yhy += sh.hy[k] * sh.g[k];
                 yhy = cta_sum(sh, yhy);
                 const double c1 = (sy + yhy) / (sy * sy);
+                /* elements (r, c) and (c, r) get the same operations on the
+                 * same values (products and the sum unfused, so no
+                 * contraction rounds the two orders differently): H stays
+                 * exactly symmetric */
                 for (int k = tid; k < n * n; k += blockDim.x) {
                     int r = k / n, c = k % n;
-                    H[k] += c1 * sh.p[r] * sh.p[c] - (sh.g[r] * sh.p[c] + sh.p[r] * sh.g[c]) / sy;
+                    const double pp = __dmul_rn(sh.p[r], sh.p[c]);
+                    const double gp = __dadd_rn(__dmul_rn(sh.g[r], sh.p[c]), __dmul_rn(sh.p[r], sh.g[c]));
+                    H[k] += c1 * pp - gp / sy;
                 }
             }
             __syncthreads();

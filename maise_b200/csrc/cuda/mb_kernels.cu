@@ -1327,6 +1327,9 @@ __global__ void k_legs(int N, int cap, const int *__restrict__ nn, int *__restri
             for (int k = 0; k < 8; k++) e[k] = k < ne ? exp(-Pg->f_eta4[p][k] * r * r) : 0.0;
             e[8] = f;
             e[9] = df / r;
+            /* with at most 7 exponents slot 7 is free: fc again, so that the
+             * forward pass reads 4 of a row's 5 16-byte pieces */
+            if (ne <= 7) e[7] = f;
             double2 *o = reinterpret_cast<double2 *>(leg + (row + dst) * MB_LEG_STRIDE);
 #pragma unroll
             for (int k = 0; k < MB_LEG_STRIDE / 2; k++) o[k] = make_double2(e[2 * k], e[2 * k + 1]);
@@ -1499,7 +1502,18 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
             const int na = seg[al], nb = seg[be], oa = seg[4 + al], ob = seg[4 + be];
             const bool tri = al == be;
             const int C = tri ? na * (na - 1) / 2 : na * nb;
-            const float tb = (float)(2 * na - 1);
+            /* the lane's candidates are c = lane, lane + 32, ...: candidate c
+             * is row r, position p of the block (row r of the strict upper
+             * triangle holds na - 1 - r pairs starting at column r + 1; a
+             * rectangular block's rows hold nb), and the cursor (r, p)
+             * moves on by 32 per candidate; it never passes the last row */
+            const int rmax = tri ? na - 2 : na - 1;
+            int r = 0, p = lane;
+            if (C > 0)
+                while (p >= (tri ? na - 1 - r : nb) && r < rmax) {
+                    p -= tri ? na - 1 - r : nb;
+                    r++;
+                }
             /* two candidate pairs per lane and iteration (c and c + 32): both
              * first hash probes are in flight together; entries are still
              * written in candidate order */
@@ -1517,18 +1531,7 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
                     jx[q] = 0u;
                     hj[q] = gh;
                     if (c < C) {
-                        int r, col;
-                        if (tri) {
-                            /* row r of the strict upper triangle starts at r (2 na - r - 1) / 2 */
-                            r = __float2int_rz(0.5f * (tb - sqrtf(fmaxf(tb * tb - 8.0f * (float)c, 0.0f))));
-                            r = min(max(r, 0), na - 2);
-                            while (r > 0 && r * (2 * na - r - 1) / 2 > c) r--;
-                            while (r < na - 2 && (r + 1) * (2 * na - r - 2) / 2 <= c) r++;
-                            col = c - r * (2 * na - r - 1) / 2 + r + 1;
-                        } else {
-                            r = c / nb;
-                            col = c - r * nb;
-                        }
+                        const int col = tri ? r + 1 + p : p;
                         const int a = oa + r, b = ob + col;
                         const double4 da = d[a], db = d[b];
                         const double dx = xsub(da.x, db.x), dy = xsub(da.y, db.y), dz = xsub(da.z, db.z);
@@ -1547,6 +1550,11 @@ __global__ void __launch_bounds__(32 * TRIP_WARPS) k_trip(int N, int cap, int tc
                                 live[q] = true;
                             }
                         }
+                    }
+                    p += 32;
+                    while (p >= (tri ? na - 1 - r : nb) && r < rmax) {
+                        p -= tri ? na - 1 - r : nb;
+                        r++;
                     }
                 }
                 uint2 e[2];
@@ -1779,7 +1787,9 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
                         const double2 *la = reinterpret_cast<const double2 *>(s.L + a * MB_LEG_STRIDE);
                         const double2 *lb = reinterpret_cast<const double2 *>(s.L + b * MB_LEG_STRIDE);
                         const double2 *lg = reinterpret_cast<const double2 *>(A.leg + (size_t)ent.y * MB_LEG_STRIDE);
-                        const double A3 = 2.0 * la[4].x * lb[4].x * __ldg(lg + 4).x;
+                        /* fc of the three legs: slot 7 when it is free (NE = 7), else slot 8 */
+                        const double A3 = NE == 7 ? 2.0 * la[3].y * lb[3].y * __ldg(lg + 3).y
+                                                  : 2.0 * la[4].x * lb[4].x * __ldg(lg + 4).x;
                         angular<NZ, NLAM>(P, c, lz, nullptr);
 #pragma unroll
                         for (int hh = 0; hh < (NE + 1) / 2; hh++) {

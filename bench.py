@@ -245,6 +245,19 @@ def population_relax(local, td, plain_sample=64, mitr=1000, fmax=0.01, urep=100.
     t_plain = time.perf_counter() - t0
     batched = len(pop) / (rb["ms"] / 1e3)
     plain_sps = plain_sample / t_plain
+    # the same launch with the reference's line-search curvature constant
+    # (0.1; the batched default is 0.5), separating the batching's gain from
+    # the line search's
+    os.environ["MAISE_B200_BATCH_SIGMA"] = "0.1"
+    try:
+        r01 = pot.relax_batch(pop, urep=urep, rlxt=3, mitr=mitr, fmax=fmax)
+    finally:
+        del os.environ["MAISE_B200_BATCH_SIGMA"]
+    at_ref = {"sigma": 0.1, "batched_structures_per_s": len(pop) / (r01["ms"] / 1e3),
+              "speedup_vs_plain": len(pop) / (r01["ms"] / 1e3) / plain_sps,
+              "evals_per_iteration": r01["evals"] / max(1, int(r01["iters"].sum())),
+              "converged": int((r01["status"] == 0).sum()),
+              "enthalpy_per_atom_median_abs_diff": float(np.median(np.abs(r01["H"] - rb["H"]) / nat))}
     pot.close()
     # FP32 roofline of k_relax_batch: the frozen counting rule over the pairs,
     # forward triplets and atom evaluations the kernel counted, over its time
@@ -265,6 +278,9 @@ def population_relax(local, td, plain_sample=64, mitr=1000, fmax=0.01, urep=100.
                             f"{nat.mean():.1f} for all",
             "batched_converged": int(conv.sum()), "plain_converged": int(sum(r["converged"] for r in plain)),
             "batched_evals": rb["evals"], "kernel_ms": rb["ms"], "roofline": roof,
+            "line_search": {"sigma": 0.5, "evals_per_iteration": rb["evals"] / max(1, int(rb["iters"].sum())),
+                            "plain_path_sigma": 0.1},
+            "at_reference_sigma": at_ref,
             "fp32_vs_fp64_ev_per_atom_max_converged": float(dE[conv].max()) if conv.any() else None,
             "fp64_max_force_converged_ev_per_a": float(f64[conv].max()) if conv.any() else None,
             "dtype": "descriptors/MLP fp32, reductions/BFGS fp64"}

@@ -261,8 +261,19 @@ class RefOracle:
         X, LAT, atmn = Oracle._prep(X, LAT, atmn)
         LAT = LAT.copy()
         counts = np.zeros(3, np.int64)
-        H = self.lib().ref_relax(self.dir, len(atmn), NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), urep, p_gpa,
-                                 rlxt, mitr, etol, counts.ctypes.data_as(_L))
+        # CELL_MIN writes its CONTCAR into the working directory: run it in a
+        # scratch directory (the model path is absolute)
+        import shutil
+        import tempfile
+        old = os.getcwd()
+        scratch = tempfile.mkdtemp(prefix="ref_relax_")
+        os.chdir(scratch)
+        try:
+            H = self.lib().ref_relax(self.dir, len(atmn), NM, ND, self.np, _ip(atmn), _dp(LAT), _dp(X), urep,
+                                     p_gpa, rlxt, mitr, etol, counts.ctypes.data_as(_L))
+        finally:
+            os.chdir(old)
+            shutil.rmtree(scratch, ignore_errors=True)
         return dict(H=H, X=X.reshape(-1, 3), LAT=LAT.reshape(3, 3), n_energy=int(counts[0]),
                     n_force=int(counts[1]), iters=int(counts[2]))
 

@@ -71,6 +71,28 @@ def test_batched_minima_are_fp64_minima(mgca, rlxt, width):
             np.testing.assert_allclose(r["LAT"][k], pop[k]["LAT"], atol=1e-12)
 
 
+@pytest.mark.parametrize("sigma", ["0.1", "0.5"])
+def test_line_search_constant(mgca, sigma, monkeypatch):
+    """The batched line search's strong Wolfe curvature constant (0.5 by
+    default; 0.1 is the reference's): either one reaches minima the FP64
+    path accepts, and the looser one takes fewer evaluations per iteration."""
+    pot, pop = mgca
+    nat = _nat(pop)
+    monkeypatch.setenv("MAISE_B200_BATCH_SIGMA", "0.1")
+    ref = pot.relax_batch(pop, urep=UREP, rlxt=3, mitr=1000, fmax=FMAX)
+    monkeypatch.setenv("MAISE_B200_BATCH_SIGMA", sigma)
+    r = pot.relax_batch(pop, urep=UREP, rlxt=3, mitr=1000, fmax=FMAX)
+    conv = np.flatnonzero(r["status"] == 0)
+    assert len(conv) >= 0.6 * len(pop)
+    for k in conv:
+        e = pot.efs(r["X"][k], r["LAT"][k], pop[k]["atmn"], ND=3, NM=300, urep=UREP)
+        assert abs(r["H"][k] - e["H"]) / nat[k] < EV_ATOM
+        assert np.abs(e["F"]).max() < FMAX + 2e-3
+    if sigma == "0.5":
+        per_iter = r["evals"] / r["iters"].sum()
+        assert per_iter < 0.8 * ref["evals"] / ref["iters"].sum()
+
+
 def test_batched_and_plain_reach_the_same_minimum(mgca):
     """Started inside one basin (a plain FP64 minimum shaken by 0.02 A), the
     batched and the plain relax end in the same minimum.  Both stop anywhere

@@ -77,19 +77,49 @@ def algorithmic_flops(basis, nspc, pairs, triplets, N):
             + N * (4 * (D * h1 + h1 * h2 + h2) + 4 * (h1 + h2)))
 
 
+def _nvml_index(local):
+    """NVML / nvidia-smi index of CUDA device `local` (CUDA_VISIBLE_DEVICES
+    renumbers the CUDA devices, not NVML's)."""
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    parts = [x.strip() for x in cvd.split(",") if x.strip()]
+    if local < len(parts) and parts[local].isdigit():
+        return int(parts[local])
+    return local
+
+
 class ClockSampler:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region:
+    NVML read every 10 ms from a thread (read-only queries), else
+    nvidia-smi every 200 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device):
-        self.device = device
+        self.device = _nvml_index(device)
         self.proc = None
+        self.nv = None
         self.lines = []
+        self.samples = []  # (sm MHz, max MHz, set of reasons) from NVML
+        self.stop_flag = threading.Event()
 
     def start(self):
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = nv.nvmlDeviceGetHandleByIndex(self.device)
+            self.bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                         nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            self._sample_nvml()
+            self.t = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
@@ -99,11 +129,41 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _sample_nvml(self):
+        nv = self.nv
+        sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        self.samples.append((float(sm), float(mx), {n for n, b in zip(self.NAMES, self.bits) if r & b}))
+
+    def _poll_nvml(self):
+        while not self.stop_flag.wait(0.01):
+            try:
+                self._sample_nvml()
+            except Exception:
+                return
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nv is not None:
+            self.stop_flag.set()
+            self.t.join(timeout=5)
+            try:
+                self._sample_nvml()
+            except Exception:
+                pass
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
+            if not self.samples:
+                return None
+            reasons = set().union(*(x[2] for x in self.samples))
+            return {"sm_mhz": float(np.median([x[0] for x in self.samples])), "sm_max_mhz": self.samples[-1][1],
+                    "reasons": sorted(reasons), "samples": len(self.samples), "source": "NVML, 10 ms"}
         if not self.proc:
             return None
         self.proc.terminate()
@@ -112,7 +172,6 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
@@ -122,12 +181,13 @@ class ClockSampler:
                 mx = float(f[2])
             except ValueError:
                 continue
-            for k, nm in enumerate(names):
+            for k, nm in enumerate(self.NAMES):
                 if f[5 + k].lower().startswith("active"):
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvidia-smi, 200 ms"}
 
 
 def max_over_ranks(seconds, dist=None):

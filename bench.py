@@ -660,7 +660,9 @@ def profile_case(case):
                  steps at the settled neighbour counts (descriptor-pass launches;
                  the autotuner's trial launches all come before the last 10)
     relax-batch  64 Mg-Ca structures of the population relax, 20 BFGS iterations
-    surrogate    features of 512 Cu-Pd-Ag offspring and 5 training epochs"""
+    surrogate    features of 512 Cu-Pd-Ag offspring and 5 training epochs
+    small-cell   the 32-atom Cu cell: 60 E+F+S passes (the autotuner's trial
+                 launches come first, then the shape it keeps)"""
     import maise_b200
     from maise_b200 import atomic_mass, maxwell, workloads
 
@@ -671,6 +673,16 @@ def profile_case(case):
         V = maxwell([atomic_mass(w["spcz"][s]) for s in w["atmn"]], 600.0, seed=7)
         st = pot.md_nvt(w["X"], w["LAT"], w["atmn"], V, 600.0, nsteps=SETTLE_STEPS, NM=100, trace=False)
         pot.md_nvt(st["X"], w["LAT"], w["atmn"], st["V"], 600.0, nsteps=10, NM=100, xi=st["xi"], trace=False)
+    elif case == "small-cell":
+        from maise_b200 import models
+
+        w = workloads.fcc_supercell(n=2, a=3.61, jitter=0.05, seed=0)
+        models.random_model(os.path.join(td, "model"), w["spcz"], models.Basis(), (w["X"], w["LAT"], w["atmn"], 3),
+                            seed=1, binding=True)
+        pot = maise_b200.Potential(os.path.join(td, "model"))
+        for _ in range(60):
+            pot.efs(w["X"], w["LAT"], w["atmn"], ND=3, NM=400)
+        print("small-cell: tuned", pot.tune_table())
     elif case == "relax-batch":
         pop = workloads.ea_population(count=64, seed=3)
         pot = maise_b200.Potential(_binding_model(td, "pop", pop, (12, 20), 5))
@@ -744,7 +756,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-population", action="store_true", help="skip the population relax and surrogate legs")
     ap.add_argument("--no-extra-legs", action="store_true", help="skip the 32-atom cell and 20000-atom particle legs")
-    ap.add_argument("--profile-case", choices=["md", "relax-batch", "surrogate"],
+    ap.add_argument("--profile-case", choices=["md", "relax-batch", "surrogate", "small-cell"],
                     help="run one small case of a hot kernel for an ncu capture and exit (no bench line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -38,9 +38,8 @@ __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a,
 /* wrap                                                                */
 /* ------------------------------------------------------------------ */
 
-__global__ void k_wrap(int N, double *__restrict__ X, mb_cell c, int *status) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
+/* JAR on atom i's position: Cartesian -> fractional, into [0, 1), back */
+__device__ __forceinline__ void wrap_atom(int i, double *__restrict__ X, const mb_cell &c, int *status) {
     double x[3];
     for (int q = 0; q < 3; q++) {
         double s = 0.0;
@@ -58,6 +57,12 @@ __global__ void k_wrap(int N, double *__restrict__ X, mb_cell c, int *status) {
         for (int j = 0; j < 3; j++) s = xadd(s, xmul(x[j], c.L[3 * j + q]));
         X[3 * i + q] = s;
     }
+}
+
+__global__ void k_wrap(int N, double *__restrict__ X, mb_cell c, int *status) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    wrap_atom(i, X, c, status);
 }
 
 /* ------------------------------------------------------------------ */
@@ -349,23 +354,41 @@ __device__ __forceinline__ void fcut_d(double rc, double r, double &f, double &d
 /* (1 + lambda c)^zeta * 2^(1-zeta) for every (zeta, lambda), and optionally
  * the derivative in c; integer zeta by repeated squaring.  NZ and NLAM are
  * upper bounds (exact for the specialised kernels); zl = z*NLAM + l. */
-template <int NZ, int NLAM>
+/* PZ = false leaves out the normalisation powz[z] = 2^(1 - zeta) (the
+ * caller folds it into the per-block grid instead: for the reference
+ * bases it is a power of two, so the results are unchanged bit for bit) */
+template <int NZ, int NLAM, bool PZ = true>
 __device__ __forceinline__ void angular(const mb_params &P, double c, double *lz, double *lzp) {
+    auto pz = [&](int z) { return PZ ? P.powz[z] : 1.0; };
     if (NZ == 4 && P.zeta_std) {
         /* zeta = 1, 2, 4, 16 (the reference bases): powers by squaring */
 #pragma unroll
         for (int l = 0; l < NLAM; l++) {
             if (l >= P.nlam) break;
             const double lam = P.lam[l], b1 = 1.0 + lam * c, b2 = b1 * b1, b4 = b2 * b2, b8 = b4 * b4;
-            lz[0 * NLAM + l] = P.powz[0] * b1;
-            lz[1 * NLAM + l] = P.powz[1] * b2;
-            lz[2 * NLAM + l] = P.powz[2] * b4;
-            lz[3 * NLAM + l] = P.powz[3] * (b8 * b8);
+            if constexpr (PZ) {
+                lz[0 * NLAM + l] = P.powz[0] * b1;
+                lz[1 * NLAM + l] = P.powz[1] * b2;
+                lz[2 * NLAM + l] = P.powz[2] * b4;
+                lz[3 * NLAM + l] = P.powz[3] * (b8 * b8);
+            } else {
+                lz[0 * NLAM + l] = b1;
+                lz[1 * NLAM + l] = b2;
+                lz[2 * NLAM + l] = b4;
+                lz[3 * NLAM + l] = b8 * b8;
+            }
             if (lzp) {
-                lzp[0 * NLAM + l] = P.powz[0] * lam;
-                lzp[1 * NLAM + l] = P.powz[1] * 2.0 * lam * b1;
-                lzp[2 * NLAM + l] = P.powz[2] * 4.0 * lam * (b2 * b1);
-                lzp[3 * NLAM + l] = P.powz[3] * 16.0 * lam * (b8 * b4 * b2 * b1);
+                if constexpr (PZ) {
+                    lzp[0 * NLAM + l] = P.powz[0] * lam;
+                    lzp[1 * NLAM + l] = P.powz[1] * 2.0 * lam * b1;
+                    lzp[2 * NLAM + l] = P.powz[2] * 4.0 * lam * (b2 * b1);
+                    lzp[3 * NLAM + l] = P.powz[3] * 16.0 * lam * (b8 * b4 * b2 * b1);
+                } else {
+                    lzp[0 * NLAM + l] = lam;
+                    lzp[1 * NLAM + l] = 2.0 * lam * b1;
+                    lzp[2 * NLAM + l] = 4.0 * lam * (b2 * b1);
+                    lzp[3 * NLAM + l] = 16.0 * lam * (b8 * b4 * b2 * b1);
+                }
             }
         }
         return;
@@ -390,15 +413,15 @@ __device__ __forceinline__ void angular(const mb_params &P, double c, double *lz
                     if (zb & (1 << k)) pw *= sq[k];
                     if (mb & (1 << k)) pm *= sq[k];
                 }
-                lz[z * NLAM + l] = P.powz[z] * pw;
-                if (lzp) lzp[z * NLAM + l] = P.powz[z] * P.zeta[z] * lam * pm;
+                lz[z * NLAM + l] = pz(z) * pw;
+                if (lzp) lzp[z * NLAM + l] = pz(z) * P.zeta[z] * lam * pm;
             }
         } else {
 #pragma unroll
             for (int z = 0; z < NZ; z++) {
                 if (z >= P.nz) break;
-                lz[z * NLAM + l] = P.powz[z] * pow(base, P.zeta[z]);
-                if (lzp) lzp[z * NLAM + l] = P.powz[z] * P.zeta[z] * lam * pow(base, P.zeta[z] - 1.0);
+                lz[z * NLAM + l] = pz(z) * pow(base, P.zeta[z]);
+                if (lzp) lzp[z * NLAM + l] = pz(z) * P.zeta[z] * lam * pow(base, P.zeta[z] - 1.0);
             }
         }
     }
@@ -1790,7 +1813,7 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
                         /* fc of the three legs: slot 7 when it is free (NE = 7), else slot 8 */
                         const double A3 = NE == 7 ? 2.0 * la[3].y * lb[3].y * __ldg(lg + 3).y
                                                   : 2.0 * la[4].x * lb[4].x * __ldg(lg + 4).x;
-                        angular<NZ, NLAM>(P, c, lz, nullptr);
+                        angular<NZ, NLAM, false>(P, c, lz, nullptr);
 #pragma unroll
                         for (int hh = 0; hh < (NE + 1) / 2; hh++) {
                             const double2 x = la[hh], y = lb[hh], z = __ldg(lg + hh);
@@ -1828,7 +1851,9 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
                 group_store64<WPA>(c0, c1, s, warp, lane);
                 {
                     const int base = P.ind4[al * al + be * be];
-                    for (int f = tid; f < P.ng4; f += NT) s.G[base + f] += s.red[g4cell[f]];
+                    /* the cells carry the zeta normalisation left out of the angular terms */
+                    for (int f = tid; f < P.ng4; f += NT)
+                        s.G[base + f] += s.red[g4cell[f]] * P.powz[(g4cell[f] & 7) >> 1];
                 }
                 group_sync<WPA>();
             }
@@ -1928,7 +1953,7 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
                 for (int t = tid; t < 64; t += NT) s.grid[t] = 0.0;
                 group_sync<WPA>();
                 for (int f = tid; f < P.ng4; f += NT)
-                    atomicAdd(&s.grid[g4cell[f]], s.G[base + f]);
+                    atomicAdd(&s.grid[g4cell[f]], s.G[base + f] * P.powz[(g4cell[f] & 7) >> 1]);
                 group_sync<WPA>();
                 auto body = [&](uint2 ent) -> double3 {
                     const int a = (int)(ent.x & 0xffu), b = (int)((ent.x >> 8) & 0xffu);
@@ -1943,7 +1968,7 @@ __global__ void __launch_bounds__(WPA * 32 * APB, (WPA >= 2 ? 512 : 384) / (WPA 
                     double lz[NZL], lzp[NZL];
 #pragma unroll
                     for (int k = 0; k < NZL; k++) { lz[k] = 0.0; lzp[k] = 0.0; }
-                    angular<NZ, NLAM>(P, c, lz, lzp);
+                    angular<NZ, NLAM, false>(P, c, lz, lzp);
                     double Q = 0.0, Qe = 0.0, Qc = 0.0;
 #pragma unroll
                     for (int hh = 0; hh < (NE + 1) / 2; hh++) {
@@ -2271,8 +2296,10 @@ __global__ void __launch_bounds__(256) k_nvt_thermostat(int N, const double *V, 
     }
 }
 
+/* the integrator, then (wrap != 0) the step's closing JAR on the moved
+ * atom, the same operations as k_wrap in one launch */
 __global__ void k_nvt_integrate(int N, double *X, double *V, const double *F, const int *spc, const double *mass,
-                                double dt, const double *out) {
+                                double dt, const double *out, mb_cell c, int wrap, int *status) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     double xi = out[9], m = mass[spc[i]];
@@ -2282,6 +2309,7 @@ __global__ void k_nvt_integrate(int N, double *X, double *V, const double *F, co
         X[3 * i + q] += v * dt + 0.5 * f * dt * dt;
         V[3 * i + q] = v + f * dt;
     }
+    if (wrap) wrap_atom(i, X, c, status);
 }
 
 __global__ void k_set_out(double *out, int idx, double v) { out[idx] = v; }
@@ -2736,8 +2764,8 @@ extern "C" int mbk_finalize(mb_dev *d, int N, int mode, double pV, void *stream,
     return (int)cudaGetLastError();
 }
 
-extern "C" int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, void *stream,
-                              long *launches) {
+extern "C" int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T,
+                              const mb_cell *c, void *stream, long *launches) {
     cudaStream_t st = (cudaStream_t)stream;
     (void)m;
     /* masses by species live after the weights in the parameter upload (see mb_core.c) */
@@ -2746,7 +2774,8 @@ extern "C" int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, do
     k_nvt_thermostat<<<nb > 0 ? nb : 1, 256, 0, st>>>(N, d->V, d->spc, mass, dt, tau, T, d->out, d->trace,
                                                       d->capTrace, d->part ? d->part + MB_RED_MAXB * 8 : nullptr,
                                                       d->ticket ? d->ticket + 1 : nullptr);
-    k_nvt_integrate<<<(N + 127) / 128, 128, 0, st>>>(N, d->X, d->V, d->F, d->spc, mass, dt, d->out);
+    k_nvt_integrate<<<(N + 127) / 128, 128, 0, st>>>(N, d->X, d->V, d->F, d->spc, mass, dt, d->out, *c,
+                                                     c->ND > 0 ? 1 : 0, d->status);
     *launches += 2;
     return (int)cudaGetLastError();
 }

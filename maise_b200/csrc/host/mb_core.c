@@ -1185,9 +1185,8 @@ static int md_step(mb_potential *p, int N, int NM, const mb_cell *c, double urep
         return cuda_fail((cudaError_t)r, "descriptor kernel");
     if ((r = mbk_finalize(&p->d, N, MB_MODE_EFS, 0.0, p->stream, &p->launches)))
         return cuda_fail((cudaError_t)r, "finalize");
-    if ((r = mbk_nvt_update(&p->d, &p->m, N, dt, tau, T / MB_KB_INV, p->stream, &p->launches)))
+    if ((r = mbk_nvt_update(&p->d, &p->m, N, dt, tau, T / MB_KB_INV, c, p->stream, &p->launches)))
         return cuda_fail((cudaError_t)r, "integrator");
-    if ((r = mbk_wrap(&p->d, N, c, p->stream, &p->launches))) return cuda_fail((cudaError_t)r, "wrap");
     if (t1) mbk_record(t1, p->stream);
     return MB_OK;
 }

@@ -173,8 +173,9 @@ int mbk_descriptor_pass(mb_dev *d, const mb_model *m, int N, int mode, double ur
 int mbk_finalize(mb_dev *d, int N, int mode, double pV, void *stream, long *launches);
 int mbk_jvp(mb_dev *d, const mb_model *m, int N, const double *dx, const double *eps, double *dG, void *stream,
             long *launches);
-int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, void *stream,
-                   long *launches);
+/* thermostat and integrator, then JAR on the moved atoms (cell c; none when c->ND <= 0) */
+int mbk_nvt_update(mb_dev *d, const mb_model *m, int N, double dt, double tau, double T, const mb_cell *c,
+                   void *stream, long *launches);
 int mbk_set_out(mb_dev *d, int idx, double v, void *stream);
 void mbk_record(void *event, void *stream);
 int mbk_shape_ready(const mb_dev *d, int N, int mode);

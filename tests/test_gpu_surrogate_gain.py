@@ -49,7 +49,7 @@ def test_screen_recalls_best_offspring_better_than_baselines(tmp_path):
     loss = sur.fit(sur.features(train), y, epochs=60, batch=256, lr=1e-3, seed=3)
     assert loss[-1] < 0.2 * loss[0]
 
-    # the judge: plain FP64 relax of every offspring of the generation
+    # the ground truth: plain FP64 relax of every offspring of the generation
     nat = np.array([len(s["atmn"]) for s in gen])
     truth = np.array([pot.relax_fmax(s["X"], s["LAT"], s["atmn"], ND=3, NM=300, urep=UREP, rlxt=3, mitr=300,
                                      fmax=FMAX)["H"] for s in gen]) / nat

@@ -5,6 +5,9 @@ exhaustively on the CPU:
   (fill_chunks in csrc/cuda/mb_kernels.cu, the candidate loop of atom_pass
   in csrc/cuda/mb_batch.cu): candidate c -> (row, col) from one FP32 square
   root, corrected by one row either way;
+* the per-lane (row, position) cursor of k_trip's candidate pairs
+  (csrc/cuda/mb_kernels.cu): lane l visits candidates l, l + 32, ... of a
+  triangular or rectangular species block, advancing the cursor by 32;
 * the lane layouts of the recursive-halving warp reductions
   (warp_reduce64f: lane l ends with cells 2l and 2l+1; warp_reduce16f:
   lanes l and l^1 end with cell (l >> 1) & 15)."""
@@ -79,3 +82,59 @@ def test_warp_reduce16_lane_layout():
     lanes = np.arange(32)
     done = out + out[lanes ^ 1]
     np.testing.assert_allclose(done, v.sum(0)[(lanes >> 1) & 15], rtol=1e-12)
+
+
+def _cursor_walk(na, nb, tri, lane):
+    """k_trip's cursor for one lane, restated: the (candidate, row, column)
+    it visits, checking on the way that every index it would use lies in
+    the block."""
+    C = na * (na - 1) // 2 if tri else na * nb
+    out = []
+    if C <= 0:
+        return out
+    rmax = na - 2 if tri else na - 1
+
+    def length(r):
+        return na - 1 - r if tri else nb
+
+    r, p = 0, lane
+    while p >= length(r) and r < rmax:
+        p -= length(r)
+        r += 1
+    c = lane
+    while c < C:
+        col = r + 1 + p if tri else p
+        assert 0 <= r <= rmax
+        assert (r + 1 <= col <= na - 1) if tri else (0 <= col <= nb - 1)
+        out.append((c, r, col))
+        c += 32
+        p += 32
+        while p >= length(r) and r < rmax:
+            p -= length(r)
+            r += 1
+    return out
+
+
+@pytest.mark.parametrize("tri", [True, False])
+def test_triplet_cursor_matches_row_major_order(tri):
+    """For every block shape up to the leg path's 128-entry capacity (all
+    triangles; rectangles up to 128 x 64 and a sample beyond), each lane's
+    cursor visits exactly the row-major candidates c = lane + 32 k, and
+    every row and column it produces lies inside the block."""
+    sizes = [(na, na) for na in range(0, 129)] if tri else \
+        [(na, nb) for na in range(0, 129) for nb in range(0, 65)] + [(na, nb) for na in (1, 7, 64, 128) for nb in
+                                                                    (65, 97, 128)]
+    for na, nb in sizes:
+        C = na * (na - 1) // 2 if tri else na * nb
+        if C <= 0:
+            continue
+        if tri:
+            r_ref, c_ref = _tri_rows_cols(na)
+        else:
+            cc = np.arange(C)
+            r_ref, c_ref = cc // nb, cc % nb
+        for lane in range(32):
+            walk = _cursor_walk(na, nb, tri, lane)
+            assert [w[0] for w in walk] == list(range(lane, C, 32))
+            for c, r, col in walk:
+                assert r == r_ref[c] and col == c_ref[c], (na, nb, lane, c)

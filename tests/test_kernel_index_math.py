@@ -8,6 +8,10 @@ exhaustively on the CPU:
 * the per-lane (row, position) cursor of k_trip's candidate pairs
   (csrc/cuda/mb_kernels.cu): lane l visits candidates l, l + 32, ... of a
   triangular or rectangular species block, advancing the cursor by 32;
+* the tensor-core staging slots of k_efs / k_efs_leg (stg_slot) and the
+  48-byte neighbour rows of k_efs_leg: a bijection onto the warp's rows,
+  and bank-conflict-free for the accesses the kernels make (32 banks of 4
+  bytes; an access of w bytes a lane served 128 / w lanes at a time);
 * the lane layouts of the recursive-halving warp reductions
   (warp_reduce64f: lane l ends with cells 2l and 2l+1; warp_reduce16f:
   lanes l and l^1 end with cell (l >> 1) & 15)."""
@@ -138,3 +142,47 @@ def test_triplet_cursor_matches_row_major_order(tri):
             assert [w[0] for w in walk] == list(range(lane, C, 32))
             for c, r, col in walk:
                 assert r == r_ref[c] and col == c_ref[c], (na, nb, lane, c)
+
+
+def _stg_slot(t, q):
+    """stg_slot in csrc/cuda/mb_kernels.cu (rows of 16 doubles)."""
+    return t * 16 + ((q + 4 * (t & 3) + ((t >> 2) & 3)) & 15)
+
+
+def _wavefronts(byte_addrs, width):
+    """Shared-memory wavefronts of one warp access of `width` bytes a lane:
+    lanes are served 128 / width at a time; within a phase, distinct 4-byte
+    words in one bank serialise (one word read by several lanes is one)."""
+    per = 128 // width
+    total = 0
+    for p in range(0, 32, per):
+        banks = {}
+        for a in byte_addrs[p:p + per]:
+            for k in range(width // 4):
+                word = a // 4 + k
+                banks.setdefault(word % 32, set()).add(word)
+        total += max(len(v) for v in banks.values())
+    return total
+
+
+def test_staging_slots_are_a_conflict_free_bijection():
+    slots = {_stg_slot(t, q) for t in range(32) for q in range(16)}
+    assert slots == set(range(32 * 16))
+    # the writes: every lane its own triplet t = lane, one value q at a time
+    for q in range(16):
+        assert _wavefronts([8 * _stg_slot(lane, q) for lane in range(32)], 8) == 2
+    # the mma operand reads: step st takes triplets 4 st + (lane & 3), value (lane >> 2) (+ 8)
+    for st in range(8):
+        for off in (0, 8):
+            assert _wavefronts([8 * _stg_slot(4 * st + (l & 3), off + (l >> 2)) for l in range(32)], 8) == 2
+
+
+def test_neighbour_rows_are_conflict_free_for_consecutive_entries():
+    """k_efs_leg's rows {x, y, z, 1/r, r, 0} (48 bytes) read as two 16-byte
+    loads: consecutive entries, as a round of consecutive list entries
+    gives the b side, take the minimum 4 wavefronts a load; a 32-byte row
+    would take 8."""
+    for base in range(0, 64):
+        for h in range(2):
+            assert _wavefronts([48 * (base + b) + 16 * h for b in range(32)], 16) == 4
+    assert _wavefronts([32 * b for b in range(32)], 16) == 8

@@ -12,6 +12,10 @@ exhaustively on the CPU:
   48-byte neighbour rows of k_efs_leg: a bijection onto the warp's rows,
   and bank-conflict-free for the accesses the kernels make (32 banks of 4
   bytes; an access of w bytes a lane served 128 / w lanes at a time);
+* the segmented warp sum of the reverse passes (leg_run_conv in
+  csrc/cuda/mb_kernels.cu, the reverse triplet stage of
+  csrc/cuda/mb_batch.cu): with equal keys contiguous within a round, the
+  first lane of each run ends with the run's total;
 * the lane layouts of the recursive-halving warp reductions
   (warp_reduce64f: lane l ends with cells 2l and 2l+1; warp_reduce16f:
   lanes l and l^1 end with cell (l >> 1) & 15)."""
@@ -186,3 +190,38 @@ def test_neighbour_rows_are_conflict_free_for_consecutive_entries():
         for h in range(2):
             assert _wavefronts([48 * (base + b) + 16 * h for b in range(32)], 16) == 4
     assert _wavefronts([32 * b for b in range(32)], 16) == 8
+
+
+def _segmented_sum(keys, vals):
+    """The kernels' doubling steps: lane l adds lane l + o's partial when
+    both hold the same key (o = 1, 2, 4, 8, 16; shfl_down leaves lanes past
+    31 their own value)."""
+    v = np.array(vals, dtype=np.float64)
+    k = list(keys)
+    for o in (1, 2, 4, 8, 16):
+        nv = v.copy()
+        for l in range(32):
+            if l + o < 32 and k[l + o] == k[l]:
+                nv[l] = v[l] + v[l + o]
+        v = nv
+    return v
+
+
+def test_segmented_warp_sum_heads_hold_their_run_totals():
+    rng = np.random.default_rng(3)
+    for _ in range(2000):
+        # a round of a row-major list: nondecreasing keys, idle lanes at the
+        # end carry keys of their own (the kernels use 256 + lane / -1 - lane)
+        n = int(rng.integers(1, 33))
+        keys = sorted(rng.integers(0, int(rng.integers(1, 12)), n).tolist()) + [1000 + l for l in range(32 - n)]
+        vals = rng.normal(size=32)
+        out = _segmented_sum(keys, vals)
+        for l in range(32):
+            if l == 0 or keys[l - 1] != keys[l]:  # the run's first lane adds it to the force
+                run = [m for m in range(l, 32) if keys[m] == keys[l]]
+                assert run == list(range(l, l + len(run)))
+                assert abs(out[l] - sum(vals[m] for m in run)) < 1e-12
+    # the order matters: a key split by another one would be counted twice
+    keys = [0, 1, 0] + [100 + l for l in range(29)]
+    out = _segmented_sum(keys, np.ones(32))
+    assert out[0] + out[2] != 2.0
